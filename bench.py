@@ -1,0 +1,321 @@
+"""Benchmark of the blocked one-sided Jacobi SVD on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the headline configuration): plain FP64 SVD of a 4096 x 2048 matrix
+with i.i.d. N(0,1) entries (PCG64 seed 1001), NPLUS = N, cycwor/cycwor tables,
+ALG 11 (block-oriented, U, V and D, innermost sorting).  One step = one full
+decomposition to convergence.  Metric: matrices per second (whole job).
+
+* value: device-resident input (the working copy is reset from an HBM copy of
+  the input inside each step), CUDA events on the library's stream around each
+  step, L2 flushed (256 MiB write) between steps outside the events;
+* e2e: the public hypJacL2 call on pinned host buffers: H2D of G, D2H of U, V
+  and D inside the timed region;
+* roofline: the block-pair kernel, algorithmic bytes per launch (768 M + 512 N
+  per block pair, 64 pairs) over its mean event-timed launch duration;
+* cpu_baseline: the CPU oracle port (OpenMP, all host threads) timed on the
+  first outer steps of the same decomposition, scaled to a whole one; DGESVJ
+  (OpenBLAS, all host threads) on the full matrix is reported beside it.
+
+N > 1: independent replicas (the single-matrix SVD is not sharded), barrier
+and max-over-ranks device time; value = matrices of all ranks / that time.
+
+--impl reference: the reference path timed on the host cores -- the CPU
+oracle port of the reference arithmetic (the reference itself is GPU code
+only) -- plus, when present, the reference's own GPU build timed once.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+M, N, ALG, SEED = 4096, 2048, 11, 1001
+N1 = N // 16
+PAIRS = N1 // 2
+STEPS1 = N1 - 1
+W = 32
+FLOP_PER_PAIR = 4 * M * W * W + 2 * N * W * W        # Gram + update of G, update of V
+BYTES_PER_PAIR = 768 * M + 512 * N                    # read G twice, write once; V read + write
+METRIC = "SVD matrices/s (4096x2048 FP64, full SVD)"
+CONFIG = {"workload": "plain FP64 SVD 4096x2048, i.i.d. N(0,1) seed 1001, NPLUS=N, cycwor/cycwor, ALG 11 "
+                      "(U, V, D), one step = one decomposition to convergence",
+          "m": M, "n": N, "alg": ALG, "strategies": "cycwor/cycwor",
+          "l2": "flushed between steps (256 MiB write, outside the timed events)"}
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region (SM clock and throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev, self.rows, self.p = dev, [], None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.p = None
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.t.join(timeout=2)
+        rows = [r for r in self.rows if len(r) >= 9]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_port_sample(G0: np.ndarray, sweeps: int, min_seconds: float = 10.0):
+    """Time the oracle port (all host threads) on the first outer steps of
+    the decomposition; scale by steps per sweep and the sweep count."""
+    from oracle import oracle as O
+    O.build()
+    from gpujachx_b200 import STRAT_PATH
+    s0 = O.load_strat(STRAT_PATH, "cycwor", 32)
+    s1 = O.load_strat(STRAT_PATH, "cycwor", N1)
+    Gf = np.array(G0, order="F", copy=True)
+    V = np.asfortranarray(np.eye(N))
+    cores = os.cpu_count() or 1
+    done, t0 = 0, time.perf_counter()
+    while done < STEPS1 and (time.perf_counter() - t0) < min_seconds:
+        O.outer_step(ALG, Gf, V, N, s0, s1, done, nthreads=cores)
+        done += 1
+    dt = time.perf_counter() - t0
+    per_matrix = dt / done * STEPS1 * sweeps
+    return {"value": 1.0 / per_matrix, "unit": "matrices/s", "cores": cores, "kind": "port",
+            "sample": f"first {done} of {STEPS1} outer steps of sweep 1 ({done * PAIRS} block pairs, "
+                      f"{dt:.1f} s), scaled x{STEPS1}/{done} steps x {sweeps} sweeps"}
+
+
+def lapack_baseline(G0: np.ndarray):
+    from oracle import lapack
+    cores = os.cpu_count() or 1
+    s, _, _, info, dt = lapack.dgesvj(G0, jobv="V", threads=cores)
+    return {"value": 1.0 / dt, "unit": "matrices/s", "cores": cores, "info": info,
+            "routine": "DGESVJ JOBA=G JOBU=U JOBV=V (OpenBLAS 0.3.30 via SciPy)", "seconds": dt}
+
+
+def ref_gpu_once(G0: np.ndarray):
+    """The reference's own hypJacL2 built for sm_100a (oracle/_ref), one run."""
+    from tests.golden.make_golden import HARNESS, case, run_ref
+    if not os.path.exists(HARNESS["base"]):
+        return None
+    c = case("bench", M, N, N, ALG, seed=SEED)
+    out = run_ref(c, G0)
+    t = out["timing"]
+    return {"s_per_matrix_wall": t[0], "s_per_matrix_compute": t[2], "sweeps": out["sweeps"],
+            "matrices_per_s_wall": 1.0 / t[0], "build": "reference sources, nvcc -arch sm_100a -DUSE_RSQRT -O3"}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from gpujachx_b200 import synth
+    G0 = synth.gaussian(M, N, SEED)
+    sweeps = int(os.environ.get("GJX_BENCH_SWEEPS", "0"))
+    ref = None
+    try:
+        ref = ref_gpu_once(G0)
+    except Exception as e:  # noqa: BLE001
+        ref = {"error": str(e)[:200]}
+    if not sweeps:
+        sweeps = (ref or {}).get("sweeps") or 10
+    vals = []
+    samples = []
+    for _ in range(args.warmup):
+        cpu_port_sample(G0, sweeps, min_seconds=2.0)
+    for _ in range(args.steps):
+        c = cpu_port_sample(G0, sweeps, min_seconds=10.0)
+        vals.append(c["value"])
+        samples.append(c)
+    v = statistics.median(vals)
+    line = {"metric": METRIC, "value": v, "unit": "matrices/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": CONFIG,
+            "cpu_baseline": dict(samples[-1], value=v),
+            "e2e": {"value": v, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference has no CPU implementation; its arithmetic is timed through the CPU oracle "
+                    "port (bit-identical restatement); ref_sm100a is the reference's own GPU code"}
+    if ref is not None:
+        line["ref_sm100a"] = ref
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baselines")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    import gpujachx_b200 as g
+    from gpujachx_b200 import synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    g.init_strats(None, "cycwor", 32, "cycwor", N1)
+    G0 = synth.gaussian(M, N, SEED)
+    dev = torch.device("cuda", local)
+    # device layout: row j of the (N, M) tensor = column j of G
+    G0d = torch.tensor(np.ascontiguousarray(G0.T), dtype=torch.float64, device=dev)
+    dG = torch.empty_like(G0d)
+    dV = torch.empty((N, N), dtype=torch.float64, device=dev)
+    dD = torch.empty(N, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        dG.copy_(G0d)
+        ret, swp, s, b = g.hypJacL2_dev(ALG, dG, N, dV, dD, stream=None)
+        return swp
+
+    for _ in range(args.warmup):
+        sweeps = step()
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local)
+    clocks.start()
+    g.profile(True)
+    barrier()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sweeps = step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    barrier()
+    prof = g.profile_read()
+    g.profile(False)
+    clk = clocks.stop()
+    total_ms = sum(times)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = t.item()
+    value = world * args.steps / (total_ms / 1000.0)
+
+    # roofline of the block-pair kernel
+    l1_mean_s = prof["l1_ms"] / max(1, prof["l1_launches"]) / 1000.0
+    hbm, peak_kind = _peaks()
+    ach = BYTES_PER_PAIR * PAIRS / l1_mean_s / 1e9
+    flops = FLOP_PER_PAIR * PAIRS / l1_mean_s / 1e12
+    roof = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+            "traffic": None, "kernel": "gjx::l1_step_kernel<true,true>",
+            "peak_kind": f"{peak_kind} HBM copy bandwidth",
+            "launch_ms": l1_mean_s * 1000.0, "launches": prof["l1_launches"],
+            "algorithmic_bytes_per_launch": BYTES_PER_PAIR * PAIRS,
+            "algorithmic_flop_per_launch": FLOP_PER_PAIR * PAIRS, "fp64_tflops": flops}
+
+    # e2e through the public host API (pinned buffers, H2D + D2H inside)
+    pin = torch.empty((N, M), dtype=torch.float64, pin_memory=True).numpy().T  # Fortran view
+    pinV = torch.empty((N, N), dtype=torch.float64, pin_memory=True).numpy().T
+    pinD = torch.empty(N, dtype=torch.float64, pin_memory=True).numpy()
+    import ctypes
+    pd = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))  # noqa: E731
+    e2e_times = []
+    L = g.lib()
+    for k in range(args.warmup + args.steps):
+        pin[...] = G0
+        sw, rs, rb = ctypes.c_uint(), ctypes.c_ulonglong(), ctypes.c_ulonglong()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ret = L.hypJacL2(ALG, M, N, N, pd(pin), M, pd(pinV), N, pd(pinD), ctypes.byref(sw), ctypes.byref(rs),
+                         ctypes.byref(rb), None)
+        dt = time.perf_counter() - t0
+        assert ret == 0, g.last_error()
+        if k >= args.warmup:
+            e2e_times.append(dt)
+    e2e_s = sum(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = t.item()
+    e2e = {"value": world * args.steps / e2e_s, "unit": "matrices/s", "h2d_bytes_per_step": M * N * 8,
+           "d2h_bytes_per_step": M * N * 8 + N * N * 8 + N * 8, "api": "hypJacL2 (host buffers, pinned)"}
+
+    line = {"metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(CONFIG, parallelism=("replicas" if world > 1 else "single GPU")),
+            "sweeps": sweeps, "e2e": e2e, "roofline": roof, "clocks": clk,
+            "gpu_launches": prof["launches"], "step_ms": times}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_port_sample(G0, sweeps)
+        try:
+            line["lapack_dgesvj"] = lapack_baseline(G0)
+        except Exception as e:  # noqa: BLE001
+            line["lapack_dgesvj"] = {"error": str(e)[:200]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,555 @@
+// gjx_host.cpp -- host side of gpujachx_b200: the strategy registry and
+// loader, the outer sweep driver, and the C ABI of include/gjx.h.
+//
+// The sweep driver follows 1/HypJacL2.cu:13-202: argument checks with the
+// same codes in the same order, V = I, then outer sweeps of one launch per
+// outer step until a sweep makes no "big" rotation (or 30 sweeps), then the
+// column normalisation that yields U and D.  Differences by design:
+//   * no host synchronisation between the steps of a sweep: the launches
+//     are queued back to back on one stream and the host reads the
+//     convergence counter (device memory, not mapped host memory) once per
+//     sweep;
+//   * errors are returned (positive codes) instead of exit();
+//   * device buffers of hypJacL2 are cached between calls
+//     (gjx_release_cache frees them).
+#include "gjx.h"
+#include "gjx_internal.h"
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <dlfcn.h>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+
+// ----------------------------------------------------------------------------
+// strategy registry (share/HypJacL.hpp:118-158, share/HypJacL.cu:11-121)
+// ----------------------------------------------------------------------------
+struct Strat {
+  bool loaded = false;
+  unsigned id0 = 0u, steps0 = 0u, pairs0 = 0u;
+  unsigned id1 = 0u, steps1 = 0u, pairs1 = 0u;
+  unsigned n0 = 0u, n1 = 0u;
+  std::vector<uint8_t> s0;  // [32][16][2], steps0 rows used
+  std::vector<uint16_t> s1; // [steps1][pairs1][2]
+  unsigned long long version = 0ull;
+};
+
+std::mutex g_mtx;
+Strat g_strat;
+int g_verbose = 1;
+
+// profiling: launch counts always; with g_prof, CUDA events around every
+// block-pair launch, read back at the end of each sweep
+struct Prof {
+  bool on = false;
+  unsigned long long launches = 0ull, l1_launches = 0ull;
+  double l1_ms = 0.0;
+  std::vector<cudaEvent_t> ev;
+} g_prof;
+thread_local std::string g_err;
+
+unsigned strat_id(const char *const name, const unsigned n, unsigned &steps)
+{
+  struct {
+    const char *name;
+    unsigned id;
+    bool quasi; // n steps instead of n - 1
+  } static const tab[] = {{"mmstep", 1u, true},  {"BrentL", 2u, false}, {"colcyc", 3u, false},
+                          {"cycloc", 4u, false}, {"rowcyc", 5u, false}, {"cycwor", 6u, false}};
+  for (const auto &t : tab)
+    if (!std::strcmp(name, t.name)) {
+      steps = t.quasi ? n : (n - 1u);
+      return t.id;
+    }
+  return 0u;
+}
+
+// the symbol "<name>%05u" (share/my_utils.cu:50-61)
+const void *strat_ptr(void *const h, const char *const snp, const unsigned n)
+{
+  char arrn[12] = {'\0'};
+  (void)std::snprintf(arrn, sizeof(arrn), "%s%05u", snp, n);
+  if (arrn[11])
+    return nullptr;
+  return dlsym(h, arrn);
+}
+
+// ----------------------------------------------------------------------------
+// per-device context: strategy tables and counters resident on the device
+// ----------------------------------------------------------------------------
+struct DevCtx {
+  bool ready = false;
+  uint8_t *d_s0 = nullptr;
+  uint16_t *d_s1 = nullptr;
+  size_t s1_cap = 0u;
+  unsigned long long version = ~0ull;
+  unsigned long long *d_cnt = nullptr; // [0] = cvg, [1] = err (int in the low word)
+  unsigned long long *h_cnt = nullptr; // pinned mirror
+  // cached matrices of hypJacL2
+  double *dG = nullptr, *dV = nullptr, *dD = nullptr;
+  size_t capG = 0u, capV = 0u, capD = 0u;
+};
+std::vector<DevCtx> g_dev;
+
+int set_cuda_error(const cudaError_t e, const char *const what)
+{
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  return GJX_ERR_CUDA;
+}
+
+#define GJX_CUDA(call, what)                                                                                         \
+  do {                                                                                                               \
+    const cudaError_t e_ = (call);                                                                                   \
+    if (e_ != cudaSuccess)                                                                                           \
+      return set_cuda_error(e_, what);                                                                               \
+  } while (0)
+
+int dev_ctx(DevCtx *&ctx)
+{
+  int dev = 0;
+  GJX_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  if ((size_t)dev >= g_dev.size())
+    g_dev.resize((size_t)dev + 1u);
+  ctx = &g_dev[(size_t)dev];
+  if (!ctx->ready) {
+    GJX_CUDA(gjx::l1_configure(), "l1_configure");
+    GJX_CUDA(cudaMalloc(&ctx->d_s0, 32u * 16u * 2u), "cudaMalloc(strat0)");
+    GJX_CUDA(cudaMalloc(&ctx->d_cnt, 2u * sizeof(unsigned long long)), "cudaMalloc(counters)");
+    GJX_CUDA(cudaHostAlloc(&ctx->h_cnt, 2u * sizeof(unsigned long long), cudaHostAllocPortable),
+             "cudaHostAlloc(counters)");
+    ctx->ready = true;
+  }
+  return 0;
+}
+
+int upload_strat(DevCtx &ctx, const cudaStream_t st)
+{
+  if (ctx.version == g_strat.version)
+    return 0;
+  const size_t need = g_strat.s1.size() * sizeof(uint16_t);
+  if (need > ctx.s1_cap) {
+    if (ctx.d_s1)
+      GJX_CUDA(cudaFree(ctx.d_s1), "cudaFree(strat1)");
+    ctx.d_s1 = nullptr;
+    GJX_CUDA(cudaMalloc(&ctx.d_s1, need), "cudaMalloc(strat1)");
+    ctx.s1_cap = need;
+  }
+  GJX_CUDA(cudaMemcpyAsync(ctx.d_s1, g_strat.s1.data(), need, cudaMemcpyHostToDevice, st), "upload strat1");
+  GJX_CUDA(cudaMemcpyAsync(ctx.d_s0, g_strat.s0.data(), g_strat.s0.size(), cudaMemcpyHostToDevice, st),
+           "upload strat0");
+  GJX_CUDA(cudaStreamSynchronize(st), "upload strategies");
+  ctx.version = g_strat.version;
+  return 0;
+}
+
+double secs(const clk::time_point a, const clk::time_point b)
+{
+  return std::chrono::duration<double>(b - a).count();
+}
+
+// The outer sweeps on device data; the caller holds g_mtx and has checked
+// the arguments.  The sweep loop of 1/HypJacL2.cu:167-216.
+int run_sweeps(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
+               double *const dG, const unsigned lddG, double *const dV, const unsigned lddV, double *const dD,
+               const cudaStream_t st, unsigned *const glbSwp, unsigned long long *const glb_s,
+               unsigned long long *const glb_b)
+{
+  if (!g_strat.loaded)
+    return GJX_ERR_NO_STRAT;
+  if (ncol / gjx::kNColB != g_strat.n1)
+    return GJX_ERR_STRAT_ORDER;
+  DevCtx *ctx = nullptr;
+  if (const int r = dev_ctx(ctx))
+    return r;
+  if (const int r = upload_strat(*ctx, st))
+    return r;
+
+  const bool cdsort = (routine & GJX_CDSORT_1) != 0u, full = (routine & GJX_FULL_SVD) != 0u,
+             blk_ori = (routine & GJX_BLK_ORI) != 0u;
+  if (full) {
+    GJX_CUDA(gjx::launch_initV(dV, ncol, lddV, st), "initV");
+    ++g_prof.launches;
+  }
+  if (g_prof.on && g_prof.ev.size() < 2u * g_strat.steps1) {
+    const size_t have = g_prof.ev.size();
+    g_prof.ev.resize(2u * g_strat.steps1);
+    for (size_t i = have; i < g_prof.ev.size(); ++i)
+      GJX_CUDA(cudaEventCreate(&g_prof.ev[i]), "cudaEventCreate");
+  }
+
+  gjx::StepParams p{};
+  p.G = dG;
+  p.V = full ? dV : nullptr;
+  p.strat1 = ctx->d_s1;
+  p.strat0 = ctx->d_s0;
+  p.cvg = ctx->d_cnt;
+  p.err = reinterpret_cast<int *>(ctx->d_cnt + 1);
+  p.ldG = lddG;
+  p.ldV = full ? lddV : 0u;
+  p.nrow = nrow;
+  p.ncol = ncol;
+  p.nplus = nplus;
+  p.pairs = g_strat.pairs1;
+  p.s0steps = g_strat.steps0;
+  p.nswp0 = blk_ori ? 1u : gjx::kNSweep;
+  p.gdefinite = (nplus ? ((nplus < ncol) ? 0 : +1) : -1);
+
+  GJX_CUDA(cudaMemsetAsync(ctx->d_cnt + 1, 0, sizeof(unsigned long long), st), "clear error word");
+  *glb_s = 0ull;
+  *glb_b = 0ull;
+  unsigned blk_swp = 0u;
+  clk::time_point ts = clk::now();
+  while (blk_swp < gjx::kNSweep) {
+    GJX_CUDA(cudaMemsetAsync(ctx->d_cnt, 0, sizeof(unsigned long long), st), "clear counter");
+    for (unsigned stp = 0u; stp < g_strat.steps1; ++stp) {
+      p.step = stp;
+      if (g_prof.on)
+        GJX_CUDA(cudaEventRecord(g_prof.ev[2u * stp], st), "cudaEventRecord");
+      GJX_CUDA(gjx::launch_l1_step(cdsort, full, p, st), "block-pair step");
+      if (g_prof.on)
+        GJX_CUDA(cudaEventRecord(g_prof.ev[2u * stp + 1u], st), "cudaEventRecord");
+    }
+    g_prof.launches += g_strat.steps1;
+    g_prof.l1_launches += g_strat.steps1;
+    ++blk_swp;
+    GJX_CUDA(cudaMemcpyAsync(ctx->h_cnt, ctx->d_cnt, 2u * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
+             "read counters");
+    GJX_CUDA(cudaStreamSynchronize(st), "sweep");
+    if (g_prof.on)
+      for (unsigned stp = 0u; stp < g_strat.steps1; ++stp) {
+        float ms = 0.0f;
+        GJX_CUDA(cudaEventElapsedTime(&ms, g_prof.ev[2u * stp], g_prof.ev[2u * stp + 1u]), "cudaEventElapsedTime");
+        g_prof.l1_ms += ms;
+      }
+    if ((int)ctx->h_cnt[1]) {
+      g_err = "a block-pair kernel timed out waiting for its tile copies";
+      return GJX_ERR_DEVICE;
+    }
+    const unsigned long long cvg = ctx->h_cnt[0];
+    const unsigned cvg_s = (unsigned)cvg, cvg_b = (unsigned)(cvg >> 32u);
+    *glb_s += cvg_s;
+    *glb_b += cvg_b;
+    const clk::time_point t2 = clk::now();
+    if (g_verbose > 0) {
+      (void)std::fprintf(stdout, "BLK_SWP(%2u), ROT_S(%10u), ROT_B(%10u), TIME(%#12.6f s)\n", blk_swp, cvg_s, cvg_b,
+                         secs(ts, t2));
+      (void)std::fflush(stdout);
+    }
+    ts = t2;
+    if (!cvg_b)
+      break;
+  }
+  *glbSwp = blk_swp;
+  GJX_CUDA(gjx::launch_initD(dG, dD, nrow, ncol, nplus, lddG, st), "initD");
+  ++g_prof.launches;
+  GJX_CUDA(cudaStreamSynchronize(st), "initD");
+  return 0;
+}
+
+// argument checks of 1/HypJacL2.cu:39-77, same codes in the same order
+int check_args(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
+               const double *const G, const unsigned ldG, const double *const V, const unsigned ldV,
+               const double *const D, const unsigned *const glbSwp, const unsigned long long *const glb_s,
+               const unsigned long long *const glb_b)
+{
+  if (routine >= 16u)
+    return -1;
+  const bool full = (routine & GJX_FULL_SVD) != 0u;
+  if (!nrow || (nrow % 64u))
+    return -2;
+  if (!ncol || (ncol > nrow) || (ncol % 32u))
+    return -3;
+  if (nplus > ncol)
+    return -4;
+  if (!G)
+    return -5;
+  if (ldG < nrow)
+    return -6;
+  if (full) {
+    if (!V)
+      return -7;
+    if (ldV < ncol)
+      return -8;
+  }
+  if (!D)
+    return -9;
+  if (!glbSwp)
+    return -10;
+  if (!glb_s)
+    return -11;
+  if (!glb_b)
+    return -12;
+  return 0;
+}
+
+template <typename T> int ensure(T *&p, size_t &cap, const size_t n, const char *const what)
+{
+  if (n <= cap)
+    return 0;
+  if (p)
+    GJX_CUDA(cudaFree(p), what);
+  p = nullptr;
+  cap = 0u;
+  GJX_CUDA(cudaMalloc(&p, n * sizeof(T)), what);
+  cap = n;
+  return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int gjx_init_strats(const char *const sdy, const char *const snp0, const unsigned n0, const char *const snp1,
+                    const unsigned n1)
+{
+  if (!sdy || !*sdy)
+    return -1;
+  if (!snp0 || !*snp0)
+    return -2;
+  if (!n0 || (n0 & 1u))
+    return -3;
+  if (!snp1 || !*snp1)
+    return -4;
+  if (!n1 || (n1 & 1u))
+    return -5;
+  unsigned steps0 = 0u, steps1 = 0u;
+  const unsigned id0 = strat_id(snp0, n0, steps0);
+  if (!id0)
+    return -6;
+  const unsigned id1 = strat_id(snp1, n1, steps1);
+  if (!id1)
+    return -7;
+  if (n0 != 32u)
+    return -11;
+  if (n1 > 1024u)
+    return -12;
+  void *const h = dlopen(sdy, RTLD_LAZY);
+  if (!h)
+    return -8;
+  const uint8_t *const a0 = static_cast<const uint8_t *>(strat_ptr(h, snp0, n0));
+  if (!a0) {
+    dlclose(h);
+    return -9;
+  }
+  const void *const a1 = strat_ptr(h, snp1, n1);
+  if (!a1) {
+    dlclose(h);
+    return -10;
+  }
+  Strat s;
+  s.id0 = id0;
+  s.steps0 = steps0;
+  s.pairs0 = n0 / 2u;
+  s.id1 = id1;
+  s.steps1 = steps1;
+  s.pairs1 = n1 / 2u;
+  s.n0 = n0;
+  s.n1 = n1;
+  s.s0.assign(32u * 16u * 2u, 0u);
+  std::memcpy(s.s0.data(), a0, (size_t)steps0 * s.pairs0 * 2u);
+  const size_t e1 = (size_t)steps1 * s.pairs1 * 2u;
+  s.s1.resize(e1);
+  if (n1 <= 256u) {
+    const uint8_t *const b = static_cast<const uint8_t *>(a1);
+    for (size_t i = 0u; i < e1; ++i)
+      s.s1[i] = b[i];
+  }
+  else
+    std::memcpy(s.s1.data(), a1, e1 * sizeof(uint16_t));
+  dlclose(h);
+  s.loaded = true;
+  std::lock_guard<std::mutex> lk(g_mtx);
+  s.version = g_strat.version + 1ull;
+  g_strat = std::move(s);
+  return 0;
+}
+
+void init_strats(const char *const sdy, const char *const snp0, const unsigned n0, const char *const snp1,
+                 const unsigned n1)
+{
+  static const char *const msg[] = {"",
+                                    "SDY empty",
+                                    "SNP0 empty",
+                                    "n0 not positive even",
+                                    "SNP1 empty",
+                                    "n1 not positive even",
+                                    "SNP0 unknown",
+                                    "SNP1 unknown",
+                                    "cannot open SDY",
+                                    "NO SUCH STRATEGY for SNP0 & n0",
+                                    "NO SUCH STRATEGY for SNP1 & n1",
+                                    "n0 must be 32",
+                                    "n1 > 1024"};
+  const int r = gjx_init_strats(sdy, snp0, n0, snp1, n1);
+  if (r) {
+    (void)std::fprintf(stderr, "[ERROR] %s(%d): %s\n", __FILE__, __LINE__, msg[-r]);
+    std::exit(EXIT_FAILURE);
+  }
+}
+
+int gjx_strat_info(unsigned *strat0, unsigned *steps0, unsigned *pairs0, unsigned *strat1, unsigned *steps1,
+                   unsigned *pairs1)
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  if (!g_strat.loaded)
+    return GJX_ERR_NO_STRAT;
+  if (strat0)
+    *strat0 = g_strat.id0;
+  if (steps0)
+    *steps0 = g_strat.steps0;
+  if (pairs0)
+    *pairs0 = g_strat.pairs0;
+  if (strat1)
+    *strat1 = g_strat.id1;
+  if (steps1)
+    *steps1 = g_strat.steps1;
+  if (pairs1)
+    *pairs1 = g_strat.pairs1;
+  return 0;
+}
+
+int gjx_get_strat1(unsigned short *out, unsigned cap)
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  if (!g_strat.loaded)
+    return -GJX_ERR_NO_STRAT;
+  const size_t n = g_strat.s1.size() < cap ? g_strat.s1.size() : cap;
+  if (out)
+    std::memcpy(out, g_strat.s1.data(), n * sizeof(unsigned short));
+  return (int)n;
+}
+
+int gjx_hypJacL2_dev(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
+                     double *const dG, const unsigned lddG, double *const dV, const unsigned lddV,
+                     double *const dD, void *const stream, unsigned *const glbSwp,
+                     unsigned long long *const glb_s, unsigned long long *const glb_b)
+{
+  if (const int r = check_args(routine, nrow, ncol, nplus, dG, lddG, dV, lddV, dD, glbSwp, glb_s, glb_b))
+    return r;
+  const bool full = (routine & GJX_FULL_SVD) != 0u;
+  if ((reinterpret_cast<uintptr_t>(dG) & 15u) || (lddG & 1u) || (reinterpret_cast<uintptr_t>(dD) & 7u) ||
+      (full && ((reinterpret_cast<uintptr_t>(dV) & 15u) || (lddV & 1u))))
+    return GJX_ERR_ALIGN;
+  std::lock_guard<std::mutex> lk(g_mtx);
+  return run_sweeps(routine, nrow, ncol, nplus, dG, lddG, dV, lddV, dD, static_cast<cudaStream_t>(stream), glbSwp,
+                    glb_s, glb_b);
+}
+
+int hypJacL2(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
+             double *const hG, const unsigned ldhG, double *const hV, const unsigned ldhV, double *const hD,
+             unsigned *const glbSwp, unsigned long long *const glb_s, unsigned long long *const glb_b,
+             double *const timing)
+{
+  const clk::time_point t0 = clk::now();
+  if (const int r = check_args(routine, nrow, ncol, nplus, hG, ldhG, hV, ldhV, hD, glbSwp, glb_s, glb_b))
+    return r;
+  const bool full = (routine & GJX_FULL_SVD) != 0u;
+  std::lock_guard<std::mutex> lk(g_mtx);
+  if (!g_strat.loaded)
+    return GJX_ERR_NO_STRAT;
+  if (ncol / gjx::kNColB != g_strat.n1)
+    return GJX_ERR_STRAT_ORDER;
+  DevCtx *ctx = nullptr;
+  if (const int r = dev_ctx(ctx))
+    return r;
+
+  const cudaStream_t st = nullptr;
+  const size_t lddG = nrow, lddV = ncol;
+  if (const int r = ensure(ctx->dG, ctx->capG, lddG * ncol, "cudaMalloc(G)"))
+    return r;
+  if (full)
+    if (const int r = ensure(ctx->dV, ctx->capV, lddV * ncol, "cudaMalloc(V)"))
+      return r;
+  if (const int r = ensure(ctx->dD, ctx->capD, (size_t)ncol, "cudaMalloc(D)"))
+    return r;
+  GJX_CUDA(cudaMemcpy2DAsync(ctx->dG, lddG * sizeof(double), hG, (size_t)ldhG * sizeof(double),
+                             (size_t)nrow * sizeof(double), ncol, cudaMemcpyHostToDevice, st),
+           "copy G to the device");
+  GJX_CUDA(cudaStreamSynchronize(st), "copy G to the device");
+  const clk::time_point t1 = clk::now();
+
+  const int r = run_sweeps(routine, nrow, ncol, nplus, ctx->dG, (unsigned)lddG, full ? ctx->dV : nullptr,
+                           (unsigned)lddV, ctx->dD, st, glbSwp, glb_s, glb_b);
+  if (r)
+    return r;
+  const clk::time_point t2 = clk::now();
+
+  GJX_CUDA(cudaMemcpy2DAsync(hG, (size_t)ldhG * sizeof(double), ctx->dG, lddG * sizeof(double),
+                             (size_t)nrow * sizeof(double), ncol, cudaMemcpyDeviceToHost, st),
+           "copy U to the host");
+  if (full)
+    GJX_CUDA(cudaMemcpy2DAsync(hV, (size_t)ldhV * sizeof(double), ctx->dV, lddV * sizeof(double),
+                               (size_t)ncol * sizeof(double), ncol, cudaMemcpyDeviceToHost, st),
+             "copy V to the host");
+  GJX_CUDA(cudaMemcpyAsync(hD, ctx->dD, (size_t)ncol * sizeof(double), cudaMemcpyDeviceToHost, st),
+           "copy D to the host");
+  GJX_CUDA(cudaStreamSynchronize(st), "copies to the host");
+  const clk::time_point t3 = clk::now();
+  if (timing) {
+    timing[0] = secs(t0, t3);
+    timing[1] = secs(t0, t1);
+    timing[2] = secs(t1, t2);
+    timing[3] = secs(t2, t3);
+  }
+  return 0;
+}
+
+void gjx_set_verbose(const int level) { g_verbose = level; }
+
+void gjx_profile(const int enable)
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  g_prof.on = (enable != 0);
+  g_prof.launches = g_prof.l1_launches = 0ull;
+  g_prof.l1_ms = 0.0;
+}
+
+void gjx_profile_read(unsigned long long *launches, unsigned long long *l1_launches, double *l1_ms)
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  if (launches)
+    *launches = g_prof.launches;
+  if (l1_launches)
+    *l1_launches = g_prof.l1_launches;
+  if (l1_ms)
+    *l1_ms = g_prof.l1_ms;
+}
+
+const char *gjx_last_error(void) { return g_err.c_str(); }
+
+const char *gjx_version(void) { return "gpujachx_b200 0.1.0 (sm_100a)"; }
+
+int gjx_release_cache(void)
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  int dev = 0;
+  GJX_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  if ((size_t)dev < g_dev.size()) {
+    DevCtx &c = g_dev[(size_t)dev];
+    if (c.dG)
+      GJX_CUDA(cudaFree(c.dG), "cudaFree");
+    if (c.dV)
+      GJX_CUDA(cudaFree(c.dV), "cudaFree");
+    if (c.dD)
+      GJX_CUDA(cudaFree(c.dD), "cudaFree");
+    c.dG = c.dV = c.dD = nullptr;
+    c.capG = c.capV = c.capD = 0u;
+  }
+  return 0;
+}
+
+int gjx_rsqrt_rn_dev(const double *in, double *out, const unsigned n)
+{
+  GJX_CUDA(gjx::launch_rsqrt_test(in, out, n, nullptr), "rsqrt_rn");
+  GJX_CUDA(cudaStreamSynchronize(nullptr), "rsqrt_rn");
+  return 0;
+}
+
+} // extern "C"

@@ -1,0 +1,43 @@
+// gjx_internal.h -- declarations shared by the host driver and the kernels.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gjx {
+
+constexpr unsigned kNColB = 16u;  // columns per block (share/HypJacL.hpp:112-116)
+constexpr unsigned kNSweep = 30u; // outer and full-block inner sweep cap (share/HypJacL.hpp:7-9)
+
+// Everything one launch of the block-pair step needs.  One CTA per block pair
+// (i, j) of outer step `step`; the pairs of a step are disjoint.
+struct StepParams {
+  double *G;                    // nrow x ncol, column major, leading dim ldG
+  double *V;                    // ncol x ncol, leading dim ldV (ACCV only)
+  const uint16_t *strat1;       // [steps1][pairs][2] block pairs (outer level)
+  const uint8_t *strat0;        // [32][16][2] column pairs (inner level)
+  unsigned long long *cvg;      // (big << 32) | small rotation counters
+  int *err;                     // device error word (bounded waits)
+  unsigned ldG, ldV, nrow, ncol, nplus;
+  unsigned pairs;               // block pairs per outer step (n1 / 2)
+  unsigned step;                // outer step index
+  unsigned s0steps;             // inner steps (31, or 32 for mmstep)
+  unsigned nswp0;               // inner sweeps per block pair (1 or 30)
+  int gdefinite;                // +1 J = I, -1 J = -I, 0 mixed signs
+};
+
+// device error codes written to *err
+enum : int { kErrWaitTimeout = 1 };
+
+size_t l1_smem_bytes();
+cudaError_t l1_configure();
+cudaError_t launch_l1_step(bool sort, bool accv, const StepParams &p, cudaStream_t s);
+cudaError_t launch_initD(double *G, double *D, unsigned nrow, unsigned ncol, unsigned nplus, unsigned ldG,
+                         cudaStream_t s);
+cudaError_t launch_initV(double *V, unsigned ncol, unsigned ldV, cudaStream_t s);
+
+// exposed for the parity tests of the primitives
+cudaError_t launch_rsqrt_test(const double *in, double *out, unsigned n, cudaStream_t s);
+
+} // namespace gjx

@@ -1,0 +1,119 @@
+/*
+ * gjx.h -- C ABI of gpujachx_b200, the B200 (sm_100a) implementation of the
+ * hierarchically blocked one-sided Jacobi SVD / hyperbolic SVD of GPUJACHx.
+ *
+ * The first two entry points are drop-in replacements of the reference's
+ * own, with the same names, arguments, return codes and side effects.  The
+ * rest is additive.  Plain pointers and sizes only; no C++ or torch types.
+ * Library: gpujachx_b200/lib/libgjx.so.
+ */
+#ifndef GJX_H
+#define GJX_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ALG / routine bits (reference share/HypJacL.hpp:88-110). */
+#define GJX_CDSORT_1 1u   /* innermost (32x32 block) sorting of the eigenvalues */
+#define GJX_FULL_SVD 2u   /* also accumulate V */
+#define GJX_ACCUMV_2 4u   /* unused by hypJacL2, as in the reference */
+#define GJX_BLK_ORI 8u    /* block-oriented: one inner sweep per block pair */
+
+/* Positive return codes (errors that are not argument errors). */
+#define GJX_ERR_CUDA 1        /* a CUDA runtime call failed: gjx_last_error() */
+#define GJX_ERR_NO_STRAT 2    /* init_strats has not loaded strategy tables */
+#define GJX_ERR_STRAT_ORDER 3 /* ncol / 16 differs from the loaded outer table order */
+#define GJX_ERR_DEVICE 4      /* a kernel reported a bounded wait that timed out */
+#define GJX_ERR_ALIGN 5       /* device pointer or leading dimension misaligned */
+
+/*
+ * Replaces hypJacL2 of 1/HypJacL2.hpp:6-27 (definition 1/HypJacL2.cu:13-202).
+ * Host memory in and out, all device memory allocated and freed per call.
+ *   routine  ALG, < 16 (bits above)
+ *   nrow     rows of G, > 0, multiple of 64
+ *   ncol     columns of G, 0 < ncol <= nrow, multiple of 32 (= 16 * n1)
+ *   nplus    number of +1 signs in J = diag(I_nplus, -I_{ncol-nplus})
+ *   hG       INOUT ldhG x ncol, column major: G in, U (unit columns) out
+ *   hV       OUT ldhV x ncol (only the first ncol rows written); routine & 2
+ *   hD       OUT ncol: D = +-||g_j||^2, the eigenvalues of G^T J G
+ *   glbSwp   OUT outer sweeps; glb_s / glb_b OUT rotations / "big" rotations
+ *   timing   OUT optional double[4]: wall, setup + H2D, compute, D2H + cleanup (s)
+ * Returns 0; -1..-12 for the reference's argument errors (same checks, same
+ * order); > 0 for the errors above.  Prints one line per outer sweep to
+ * stdout like the reference, unless gjx_set_verbose(0).
+ */
+int hypJacL2(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
+             double *const hG, const unsigned ldhG, double *const hV, const unsigned ldhV, double *const hD,
+             unsigned *const glbSwp, unsigned long long *const glb_s, unsigned long long *const glb_b,
+             double *const timing);
+
+/*
+ * Replaces init_strats of share/HypJacL.hpp:206 (definition
+ * share/HypJacL.cu:11-121): loads the inner (snp0, n0 = 32 columns) and outer
+ * (snp1, n1 = ncol / 16 blocks) strategy tables "<name>%05u" from the shared
+ * library sdy (strat.so), bytes for n <= 256, uint16 above.  Names: mmstep,
+ * BrentL, colcyc, cycloc, rowcyc, cycwor.  On failure it prints "[ERROR] ..."
+ * and exits the process, as the reference does; gjx_init_strats reports the
+ * same failures as a return code instead.
+ */
+void init_strats(const char *const sdy, const char *const snp0, const unsigned n0, const char *const snp1,
+                 const unsigned n1);
+
+/* As init_strats, returning 0 or a negative code instead of exiting:
+ * -1 empty sdy, -2 empty snp0, -3 n0 not positive even, -4 empty snp1,
+ * -5 n1 not positive even, -6 unknown snp0, -7 unknown snp1, -8 dlopen
+ * failed, -9 no table for snp0 & n0, -10 no table for snp1 & n1,
+ * -11 n0 != 32 (the inner level is 32 columns), -12 n1 > 1024. */
+int gjx_init_strats(const char *const sdy, const char *const snp0, const unsigned n0, const char *const snp1,
+                    const unsigned n1);
+
+/* Loaded strategy state: ids (share/HypJacL.hpp:118-158), steps, pairs. */
+int gjx_strat_info(unsigned *strat0, unsigned *steps0, unsigned *pairs0, unsigned *strat1, unsigned *steps1,
+                   unsigned *pairs1);
+/* Copy of the loaded outer table, [steps1][pairs1][2] uint16; returns the
+ * number of entries copied (<= cap), or < 0. */
+int gjx_get_strat1(unsigned short *out, unsigned cap);
+
+/*
+ * hypJacL2 on device-resident data (no host copies, no per-call allocation
+ * of the matrices): dG (lddG >= nrow), dV (lddV >= ncol, routine & 2), dD
+ * device pointers, 16-byte aligned, lddG and lddV even.  V is set to I here.
+ * stream is a cudaStream_t (NULL = legacy default stream).  Blocks until the
+ * result is ready.  Same return codes as hypJacL2.
+ */
+int gjx_hypJacL2_dev(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
+                     double *const dG, const unsigned lddG, double *const dV, const unsigned lddV,
+                     double *const dD, void *const stream, unsigned *const glbSwp,
+                     unsigned long long *const glb_s, unsigned long long *const glb_b);
+
+/* Frees the device buffers that hypJacL2 keeps between calls on the current
+ * device (they are reused by the next call of the same or smaller size). */
+int gjx_release_cache(void);
+
+/* 0: silent; 1 (default): per-sweep lines on stdout like the reference. */
+void gjx_set_verbose(const int level);
+
+/* Profiling.  gjx_profile(1) resets the counters and times every block-pair
+ * kernel launch with CUDA events on its stream; gjx_profile(0) resets and
+ * stops timing (launch counts are always kept).  gjx_profile_read returns the
+ * kernel launches since the reset (all kernels of this library), the
+ * block-pair launches among them, and their summed device time in ms. */
+void gjx_profile(const int enable);
+void gjx_profile_read(unsigned long long *launches, unsigned long long *l1_launches, double *l1_ms);
+
+/* Message of the last GJX_ERR_CUDA / GJX_ERR_DEVICE in this thread. */
+const char *gjx_last_error(void);
+
+/* Library version string. */
+const char *gjx_version(void);
+
+/* Device check of the correctly rounded 1/sqrt: out[i] = rsqrt_rn(in[i]) for
+ * device arrays; returns 0 or GJX_ERR_CUDA. */
+int gjx_rsqrt_rn_dev(const double *in, double *out, const unsigned n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GJX_H */

@@ -1,0 +1,70 @@
+"""CPU checks of the strategy tables and of the loader (share/HypJacL.cu:11-121).
+
+Every table of strat.so must be a valid parallel ordering (disjoint pairs in
+each step, p < q, complete coverage); the product loader (gjx_init_strats)
+must read exactly what the oracle's restatement of the reference loader reads.
+"""
+
+import ctypes
+import itertools
+
+import numpy as np
+import pytest
+
+FAMILIES = ("mmstep", "BrentL", "colcyc", "cycloc", "rowcyc", "cycwor")
+
+
+def _orders(strat_path):
+    lib = ctypes.CDLL(strat_path)
+    out = []
+    for fam in FAMILIES:
+        for n in range(2, 1025, 2):
+            try:
+                getattr(lib, "%s%05d" % (fam, n))
+            except AttributeError:
+                continue
+            out.append((fam, n))
+    return out
+
+
+def test_table_count(strat_path):
+    o = _orders(strat_path)
+    assert len(o) == 325  # every shipped header; 00960 and 01024 are absent upstream
+    assert max(n for _, n in o) == 896
+
+
+def test_every_table_is_a_parallel_ordering(strat_path, oracle):
+    for fam, n in _orders(strat_path):
+        t = oracle.load_strat(strat_path, fam, n).astype(np.int64)
+        steps = t.shape[0]
+        assert steps == (n if fam == "mmstep" else n - 1), (fam, n)
+        assert np.all(t[..., 0] < t[..., 1]), (fam, n)
+        assert t.max() < n
+        for s in range(steps):
+            flat = t[s].ravel()
+            assert len(np.unique(flat)) == n, (fam, n, s)  # disjoint, all indices
+        pairs = set(map(tuple, t.reshape(-1, 2).tolist()))
+        assert len(pairs) == n * (n - 1) // 2, (fam, n)  # every pair at least once
+
+
+def test_product_loader_matches_oracle(built, oracle):
+    import gpujachx_b200 as g
+    for fam, n1 in [("cycwor", 16), ("cycwor", 512), ("rowcyc", 24), ("colcyc", 896), ("BrentL", 64),
+                    ("cycloc", 256), ("mmstep", 288)]:
+        g.init_strats(built["strat"], "cycwor", 32, fam, n1)
+        ours = g.strat1_table()
+        ref = oracle.load_strat(built["strat"], fam, n1)
+        assert ours.dtype == np.uint16 and np.array_equal(ours, ref), (fam, n1)
+        info = g.strat_info()
+        assert info["steps1"] == ref.shape[0] and info["pairs1"] == n1 // 2
+        assert info["strat0"] == 6 and info["steps0"] == 31
+
+
+def test_strategy_ids(built):
+    import gpujachx_b200 as g
+    ids = {"mmstep": 1, "BrentL": 2, "colcyc": 3, "cycloc": 4, "rowcyc": 5, "cycwor": 6}
+    for fam, i in ids.items():
+        g.init_strats(built["strat"], fam, 32, fam, 16)
+        info = g.strat_info()
+        assert info["strat0"] == i and info["strat1"] == i
+        assert info["steps0"] == (32 if fam == "mmstep" else 31)
