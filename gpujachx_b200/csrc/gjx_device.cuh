@@ -41,14 +41,34 @@ __device__ __forceinline__ bool above_mid(const unsigned long long y2p1, const u
   return T_hi < (1ull << 32);                            // (P * F) >> 64 < 2^96
 }
 
-// 1/sqrt(a) rounded to nearest.  Our own method: a = F * 2^e, e even,
-// F in [2^52, 2^54); 1/sqrt(F) = Y * 2^-79 with a 53-bit Y is bracketed by an
-// estimate from two correctly rounded operations and fixed by exact integer
-// tests of the rounding midpoints (the sign of 1 - m^2 F).  Any correctly
-// rounded 1/sqrt returns these bits.
+// 2^k as a double, k in [-1022, 1023]
+__device__ __forceinline__ double pow2(const int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
+
+// 1/sqrt(a) rounded to nearest.  Our own method.  Scale a = f * 4^k with
+// f in [1, 4), so that 1/sqrt(f) = Y * 2^-53 lies in (1/2, 1) with Y a
+// 53-bit integer after rounding.  From the hardware-assisted estimate y:
+//   * fast path (after P. Markstein, "IA-64 and Elementary Functions"):
+//     e = 1 - f y^2 by two FMAs on y^2 = yh + yl (error below 2^-103), then
+//     1/sqrt(f) = y (1 + e/2 + O(e^2)); in ulps the correction is
+//     d = 2^53 y e / 2 within 2^-48, so Y = y 2^53 + rint(d) unless d lies
+//     within 2^-40 of a half-integer;
+//   * otherwise (almost never), the exact test: 1/sqrt(f) lies above the
+//     midpoint (2Y+1) * 2^-54 iff (2Y+1)^2 * F < 2^160, F = f 2^52, decided
+//     in integers.
+// Any correctly rounded 1/sqrt returns these bits.
+__device__ __noinline__ long long rsqrt_fix_exact(long long Y, const unsigned long long F)
+{
+  for (int i = 0; (i < 4) && above_mid((unsigned long long)(2 * Y + 1), F); ++i)
+    ++Y;
+  for (int i = 0; (i < 4) && (Y > (1ll << 52)) && !above_mid((unsigned long long)(2 * Y - 1), F); ++i)
+    --Y;
+  return Y;
+}
+
 __device__ __forceinline__ double rsqrt_rn(const double a)
 {
-  if (!(a > 0.0) || isinf(a)) {
+  unsigned long long bits = (unsigned long long)__double_as_longlong(a);
+  if ((bits >> 63) || ((bits >> 52) == 0x7FFu) || !(bits << 1)) { // negative, inf, nan, zero
     if (isnan(a))
       return a + a;
     if (a == 0.0)
@@ -57,35 +77,32 @@ __device__ __forceinline__ double rsqrt_rn(const double a)
       return __longlong_as_double((long long)0xfff8000000000000ull);
     return 0.0; // +inf
   }
-  const unsigned long long bits = (unsigned long long)__double_as_longlong(a);
-  int E = (int)((bits >> 52) & 0x7FFu);
-  unsigned long long F = bits & 0xFFFFFFFFFFFFFull;
-  if (E)
-    F |= (1ull << 52);
-  else {
-    const int sh = __clzll((long long)F) - 11;
-    F <<= sh;
-    E = 1 - sh;
+  int sh = 0; // a = a' * 2^-sh with a' normal
+  double an = a;
+  if (!(bits >> 52)) {
+    an = a * pow2(108);
+    bits = (unsigned long long)__double_as_longlong(an);
+    sh = 108;
   }
-  int e = E - 1075;
-  if (e & 1) {
-    F <<= 1;
-    --e;
+  const double ya = rsqrt(an);              // estimate of 1/sqrt(a'), within an ulp
+  const int eu = (int)(bits >> 52) - 1023; // a' = m * 2^eu, m in [1, 2)
+  const int k2 = eu & ~1;                  // a' = f * 2^k2, f in [1, 4)
+  const double f = __longlong_as_double((long long)((bits & 0xFFFFFFFFFFFFFull) | ((unsigned long long)(1023 + (eu - k2)) << 52)));
+  const int kk = (k2 - sh) / 2; // a = f * 4^kk exactly (k2 - sh is even)
+  if (f == 1.0)
+    return pow2(-kk);
+  const double y = ya * pow2(k2 / 2); // estimate of 1/sqrt(f), in (1/2, 1] (exact scaling)
+  const double yh = y * y;
+  const double yl = __fma_rn(y, y, -yh);
+  const double e = __fma_rn(-f, yl, __fma_rn(-f, yh, 1.0));
+  const double d = (y * (0.5 * e)) * pow2(53);
+  const double dr = rint(d);
+  double Yd = __fma_rn(y, pow2(53), dr); // y 2^53 + rint(d): an integer below 2^54, exact
+  if (fabs(d - dr) > 0.5 - 0x1.0p-40 || Yd >= pow2(53) || Yd < pow2(52)) {
+    long long Y = (long long)fmin(fmax(Yd, pow2(52)), pow2(53) - 1.0);
+    Yd = (double)rsqrt_fix_exact(Y, (unsigned long long)(f * pow2(52)));
   }
-  if (F == (1ull << 52))
-    return scalbn(1.0, -26 - e / 2);
-  const double est = __drcp_rn(__dsqrt_rn(__ull2double_rn(F)));
-  long long Y = __double2ll_rz(scalbn(est, 79));
-  if (Y >= (1ll << 53))
-    Y = (1ll << 53) - 1;
-  if (Y < (1ll << 52))
-    Y = (1ll << 52);
-  // the estimate is within two ulps: at most a few corrections, bounded
-  for (int i = 0; (i < 4) && above_mid((unsigned long long)(2 * Y + 1), F); ++i)
-    ++Y;
-  for (int i = 0; (i < 4) && (Y > (1ll << 52)) && !above_mid((unsigned long long)(2 * Y - 1), F); ++i)
-    --Y;
-  return scalbn(__ll2double_rn(Y), -79 - e / 2);
+  return Yd * pow2(-53 - kk); // exact scaling into the normal range
 }
 
 // ---------------------------------------------------------------------------
@@ -106,29 +123,21 @@ __device__ __forceinline__ double sum32(double v)
 // 2x2 rotations (share/device_code_common_rotate.hpp:16-64, USE_RSQRT form).
 // Return 1 for a "big" rotation (c != 1), 0 otherwise.
 // ---------------------------------------------------------------------------
+// The three cases of each are evaluated without branching (the operands of
+// the case that applies are selected, then the same operations run), so the
+// 16 lanes that compute 16 rotations at once never diverge.
 __device__ __forceinline__ int rotT(const double Apq, const double Dp, const double Dq, double &c, double &t)
 {
   const double h = Dq - Dp;
   const double ct2 = __ddiv_rn(h, Apq * 2.0);
   const double CT2 = fabs(ct2);
-  if (CT2 < kSqrtHeps) {
-    const double cot = CT2 + 1.0;
-    t = copysign(__drcp_rn(cot), ct2);
-    c = rsqrt_rn(__fma_rn(t, t, 1.0));
-    return 1;
-  }
-  else if (CT2 >= kSqrt2Heps) {
-    const double cot = CT2 * 2.0;
-    c = 1.0;
-    t = copysign(__drcp_rn(cot), ct2);
-    return 0;
-  }
-  else {
-    const double cot = CT2 + __dsqrt_rn(__fma_rn(CT2, CT2, 1.0));
-    t = copysign(__drcp_rn(cot), ct2);
-    c = rsqrt_rn(__fma_rn(t, t, 1.0));
-    return (c < 1.0);
-  }
+  const bool small = CT2 < kSqrtHeps, large = CT2 >= kSqrt2Heps;
+  const double cot_mid = CT2 + __dsqrt_rn(__fma_rn(CT2, CT2, 1.0));
+  const double cot = small ? (CT2 + 1.0) : (large ? (CT2 * 2.0) : cot_mid);
+  t = copysign(__drcp_rn(cot), ct2);
+  const double cr = rsqrt_rn(__fma_rn(t, t, 1.0));
+  c = large ? 1.0 : cr;
+  return small ? 1 : (large ? 0 : (cr < 1.0));
 }
 
 __device__ __forceinline__ int rotH(const double Apq, const double Dp, const double Dq, double &c, double &t)
@@ -136,23 +145,14 @@ __device__ __forceinline__ int rotH(const double Apq, const double Dp, const dou
   const double h = Dq + Dp;
   const double ct2 = -__ddiv_rn(h, Apq * 2.0);
   const double CT2 = fabs(ct2);
-  if (CT2 >= kSqrt2Heps) {
-    const double cot = CT2 * 2.0;
-    c = 1.0;
-    t = copysign(__drcp_rn(cot), ct2);
-    return 0;
-  }
-  else if (CT2 > 1.0) {
-    const double cot = CT2 + __dsqrt_rn(__fma_rn(CT2, CT2, -1.0));
-    t = copysign(__drcp_rn(cot), ct2);
-    c = rsqrt_rn(__fma_rn(-t, t, 1.0));
-    return (c > 1.0);
-  }
-  else {
-    c = kCoshIFix;
-    t = kTanh1Fix;
-    return 1;
-  }
+  const bool large = CT2 >= kSqrt2Heps, mid = !large && (CT2 > 1.0);
+  const double cot_mid = CT2 + __dsqrt_rn(__fma_rn(CT2, CT2, -1.0));
+  const double cot = large ? (CT2 * 2.0) : cot_mid;
+  const double tt = copysign(__drcp_rn(cot), ct2);
+  const double cr = rsqrt_rn(__fma_rn(-tt, tt, 1.0));
+  c = large ? 1.0 : (mid ? cr : kCoshIFix);
+  t = (large || mid) ? tt : kTanh1Fix;
+  return large ? 0 : (mid ? (cr > 1.0) : 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -213,6 +213,32 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, const uint3
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    smem_u32(dst)),
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// 16-byte asynchronous copy global -> shared (both 16-byte aligned), L2 only
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+// one arrival on the mbarrier once all prior cp.async of this thread completed
+__device__ __forceinline__ void cp_async_arrive(uint64_t *bar)
+{
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// TMA tensor copy of a 3-D box at (c0, c1, c2) of the tensor map (kernel
+// parameter space) into shared memory, completing bytes on the mbarrier.
+// c0 * element size must be a multiple of 16 bytes (c0 = 0 here).
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *tm, const int c0, const int c1,
+                                            const int c2, uint64_t *bar)
+{
+  asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+               "[%5];" ::"r"(smem_u32(dst)),
+               "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
                : "memory");
 }
 

@@ -200,6 +200,10 @@ int run_sweeps(const unsigned routine, const unsigned nrow, const unsigned ncol,
   p.s0steps = g_strat.steps0;
   p.nswp0 = blk_ori ? 1u : gjx::kNSweep;
   p.gdefinite = (nplus ? ((nplus < ncol) ? 0 : +1) : -1);
+  p.split = gjx::l1_split(p.pairs);
+  GJX_CUDA(gjx::make_update_map(&p.tmG, dG, nrow, ncol, lddG), "tensor map of G");
+  if (full)
+    GJX_CUDA(gjx::make_update_map(&p.tmV, dV, ncol, ncol, lddV), "tensor map of V");
 
   GJX_CUDA(cudaMemsetAsync(ctx->d_cnt + 1, 0, sizeof(unsigned long long), st), "clear error word");
   *glb_s = 0ull;

@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace gjx {
@@ -12,7 +13,9 @@ constexpr unsigned kNSweep = 30u; // outer and full-block inner sweep cap (share
 
 // Everything one launch of the block-pair step needs.  One CTA per block pair
 // (i, j) of outer step `step`; the pairs of a step are disjoint.
-struct StepParams {
+struct alignas(64) StepParams {
+  CUtensorMap tmG;              // 3-D view (32 rows, nrow/32 pieces, ncol columns) of G
+  CUtensorMap tmV;              // the same of V (ACCV only)
   double *G;                    // nrow x ncol, column major, leading dim ldG
   double *V;                    // ncol x ncol, leading dim ldV (ACCV only)
   const uint16_t *strat1;       // [steps1][pairs][2] block pairs (outer level)
@@ -25,7 +28,11 @@ struct StepParams {
   unsigned s0steps;             // inner steps (31, or 32 for mmstep)
   unsigned nswp0;               // inner sweeps per block pair (1 or 30)
   int gdefinite;                // +1 J = I, -1 J = -I, 0 mixed signs
+  unsigned split;               // CTAs per block pair (a cluster): 1 or 2
 };
+
+// TMA tensor maps for the update staging (3-D view, box {34, 8, 16}); 0 or a CUDA error
+cudaError_t make_update_map(CUtensorMap *tm, const double *base, unsigned nrow, unsigned ncol, unsigned ld);
 
 // device error codes written to *err
 enum : int { kErrWaitTimeout = 1 };
@@ -33,6 +40,8 @@ enum : int { kErrWaitTimeout = 1 };
 size_t l1_smem_bytes();
 cudaError_t l1_configure();
 cudaError_t launch_l1_step(bool sort, bool accv, const StepParams &p, cudaStream_t s);
+// CTAs per block pair for `pairs` pairs per step on the current device
+unsigned l1_split(unsigned pairs);
 cudaError_t launch_initD(double *G, double *D, unsigned nrow, unsigned ncol, unsigned nplus, unsigned ldG,
                          cudaStream_t s);
 cudaError_t launch_initV(double *V, unsigned ncol, unsigned ldV, cudaStream_t s);

@@ -1,247 +1,366 @@
 // gjx_kernels.cu -- sm_100a kernels of the blocked one-sided Jacobi (H)SVD.
 //
-// One CTA of 512 threads processes one block pair (i, j) of an outer step:
+// One block pair (i, j) of an outer step is processed by a cluster of NSPLIT
+// CTAs (NSPLIT = 2 when the step has few pairs, so that both SMs of a pair
+// work on it; 1 when the pairs already fill the GPU), 256 threads each:
 //
-//   1. Gram matrix of the M x 32 column pair [G_i G_j] (lower triangle only:
-//      the Cholesky never reads the upper one), streamed through shared
-//      memory in 64-row tiles by the TMA engine (cp.async.bulk + mbarrier,
-//      4 stages); each of the 528 entries is one FMA chain in the
-//      reference's row order (share/device_code_common_Cholesky.hpp:4-56),
-//      computed in 4x4 register tiles with a sliding row window;
-//   2. 32x32 Cholesky in one warp, rows in registers, shuffles for the
-//      pivots (share/device_code_common_Cholesky.hpp:58-158);
-//   3. inner Jacobi sweep(s) over the 32 columns of R, one warp per column
-//      pair, warp-shuffle dot products, trigonometric or hyperbolic
-//      rotations, optional KISS sorting (share/device_code_nosort.hpp,
-//      share/device_code_cdsort.hpp, share/device_code_cdsort_KISS.hpp);
-//   4. [G_i G_j] <- [G_i G_j] V_loc (and V likewise), 256-row stages
-//      brought in by the TMA engine, each output a 32-FMA chain in the
-//      reference's skewed order (share/device_code_common.hpp:146-185),
-//      computed in 4x8 register tiles along anti-diagonals.
+//   1. Gram matrix of the M x 32 column pair [G_i G_j], lower triangle only
+//      (the Cholesky never reads the upper one).  Each CTA streams the whole
+//      pair through shared memory in 64-row tiles with the TMA engine
+//      (cp.async.bulk + mbarrier, 4 stages) and computes its share of the
+//      528 entries; every entry is one FMA chain in the reference's row
+//      order (share/device_code_common_Cholesky.hpp:4-56), computed in 2x2
+//      register tiles with a sliding row window.  The shares are exchanged
+//      through distributed shared memory, then one cluster barrier.
+//   2. 32x32 Cholesky in one warp, rows in registers, pivots by shuffles
+//      (share/device_code_common_Cholesky.hpp:58-158).
+//   3. Inner Jacobi sweep(s) on R: each warp owns two column pairs of each
+//      inner step, lane x row x; warp-shuffle dot products in the
+//      reference's butterfly order, trigonometric or hyperbolic rotations,
+//      optional KISS sorting (share/device_code_nosort.hpp,
+//      share/device_code_cdsort.hpp, share/device_code_cdsort_KISS.hpp).
+//      Steps 2 and 3 are deterministic, so every CTA of the cluster
+//      computes them itself and holds the same V_loc bit for bit.
+//   4. [G_i G_j] <- [G_i G_j] V_loc (and V likewise): 256-row stages brought
+//      in by the TMA engine, the stages dealt out to the CTAs of the
+//      cluster; each output is a 32-FMA chain in the reference's skewed
+//      order (share/device_code_common.hpp:146-185), computed in 4x8
+//      register tiles along anti-diagonals.
 //
 // All arithmetic is in the reference's order, so results are bit-identical.
+#include <cooperative_groups.h>
+#include <cudaTypedefs.h>
+
 #include "gjx_device.cuh"
 #include "gjx_internal.h"
 
+namespace cg = cooperative_groups;
+
 namespace gjx {
 
-constexpr unsigned kThreads = 512u;
+constexpr unsigned kThreads = 256u;
 constexpr long long kWaitLimit = 2000000000ll; // ~1 s of cycles per wait
 
-// Gram staging: column c of a 64-row tile at gcol_off(c), rows 0..95 where
-// rows 64..95 repeat rows 0..31, so a chain starting at row x never wraps.
-constexpr unsigned kGramStages = 4u;
-constexpr unsigned kGramColLd = 112u;
+// Gram staging: a stage holds 2 tiles of 64 rows of the 32 columns; tile t
+// of column c at gcol_off(c) + 96 t, rows 0..95 where rows 64..95 repeat
+// rows 0..31, so a chain starting at tile row x reads rows x..x+63 without
+// wrapping.  Filled by 16-byte cp.async (the layout needs 16-byte placement
+// freedom: repeated rows and per-column bank offsets), 3 stages in flight.
+constexpr unsigned kGramTiles = 2u;
+constexpr unsigned kGramStages = 3u;
+constexpr unsigned kGramColLd = 2u * 96u + 16u;
 constexpr unsigned kGramStage = 32u * kGramColLd; // doubles
-constexpr uint32_t kGramTxBytes = 32u * (512u + 256u);
-__device__ __forceinline__ unsigned gcol_off(const unsigned c) { return c * kGramColLd + 2u * ((c >> 2) & 7u); }
+constexpr unsigned kGramChunks = 48u;             // 16-byte chunks per column and tile
+__device__ __forceinline__ unsigned gcol_off(const unsigned c) { return c * kGramColLd + 2u * ((c >> 1) & 7u); }
 
-// Update staging: 256 rows x 32 columns; the 32-row piece p of a column
-// starts at p*34 (2 doubles of skew per piece spreads the banks).
+// Update staging: 256 rows x 32 columns; the 32-row piece p of column c
+// starts at c*272 + p*34 (2 doubles of skew per piece spread the banks).
+// One TMA tensor copy per block and stage: a 3-D view (32 rows, pieces,
+// columns) of the matrix and a box of {34, 8, 16} lands exactly in this
+// layout (rows 32 and 33 of a piece box lie outside the view: zero fill).
 constexpr unsigned kUpdRows = 256u;
 constexpr unsigned kUpdColLd = 272u;
 constexpr unsigned kUpdStages = 2u;
 constexpr unsigned kUpdStage = 32u * kUpdColLd; // doubles
 constexpr unsigned kVTLd = 34u;                 // B^T rows (V_loc transposed)
+constexpr uint32_t kUpdBoxBytes = 34u * 8u * 16u * 8u;
 
 constexpr unsigned kRegion =
     (kGramStages * kGramStage > kUpdStages * kUpdStage) ? kGramStages * kGramStage : kUpdStages * kUpdStage;
 
-// shared memory map (doubles, then bytes)
+// one inner rotation, as phase B of an inner step leaves it for phase C
+struct Rot {
+  double c, t, t_;
+  int mode; // 0 nothing, 1 rotate, 2 swap columns
+  int scale, swap;
+};
+
+// shared memory map (in doubles)
 constexpr unsigned kOffR = kRegion;        // R, 32x32 (later B^T, 32x34)
 constexpr unsigned kOffVl = kOffR + 32u * kVTLd;
 constexpr unsigned kOffS0 = kOffVl + 1024u; // strat0 copy, 1024 bytes
 constexpr unsigned kOffRed = kOffS0 + 128u; // 32 unsigned
 constexpr unsigned kOffBar = kOffRed + 16u; // 8 mbarriers
-constexpr unsigned kOffFlag = kOffBar + 8u;
-constexpr unsigned kSmemDoubles = kOffFlag + 2u;
+constexpr unsigned kOffProd = kOffBar + 8u;          // 16 pairs x 3 products x 33
+constexpr unsigned kOffRots = kOffProd + 16u * 3u * 33u; // 16 Rot
+constexpr unsigned kSmemDoubles = kOffRots + 16u * (sizeof(Rot) / 8u);
 
 size_t l1_smem_bytes() { return (size_t)kSmemDoubles * sizeof(double); }
 
 #define E32(A, r, c) (A)[(c) * 32u + (r)]
 
 // ---------------------------------------------------------------------------
-// Gram: one 64-row tile for the thread's 4x4 block of entries (x0+u, y0+v).
-// Entry (x, y) adds G[r,y]*G[r,x] for r = x, x+1, ..., x+63 (mod 64).
+// Gram: one 64-row tile (at row base of the stage) for a 2x2 block of entries
+// (x0+u, y0+v).  Entry (x, y) adds G[r,y]*G[r,x] for r = x, x+1, ..., x+63
+// (mod 64), the reference's order.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void gram_tile(const double *const st, const unsigned x0, const unsigned y0,
-                                          double (&acc)[4][4])
+__device__ __forceinline__ void gram_tile(const double *const st, const unsigned base, const unsigned x0,
+                                          const unsigned y0, double (&acc)[2][2])
 {
-  const double *xp[4], *yp[4];
-#pragma unroll
-  for (unsigned u = 0u; u < 4u; ++u)
-    xp[u] = st + gcol_off(x0 + u) + x0 + u;
-#pragma unroll
-  for (unsigned v = 0u; v < 4u; ++v)
-    yp[v] = st + gcol_off(y0 + v) + x0;
-  double W[4][4]; // W[slot][v]: row x0 + (j..j+3), slot = row mod 4
-#pragma unroll
-  for (unsigned m = 0u; m < 4u; ++m)
-#pragma unroll
-    for (unsigned v = 0u; v < 4u; ++v)
-      W[m][v] = yp[v][m];
+  const double *const xp0 = st + gcol_off(x0) + base + x0;
+  const double *const xp1 = st + gcol_off(x0 + 1u) + base + x0 + 1u;
+  const double *const yp0 = st + gcol_off(y0) + base + x0;
+  const double *const yp1 = st + gcol_off(y0 + 1u) + base + x0;
+  double W[2][2]; // W[slot][v]: rows x0 + j, x0 + j + 1; slot = row parity
+  W[0][0] = yp0[0];
+  W[0][1] = yp1[0];
+  W[1][0] = yp0[1];
+  W[1][1] = yp1[1];
 #pragma unroll
   for (unsigned j = 0u; j < 64u; ++j) {
-    double X[4];
-#pragma unroll
-    for (unsigned u = 0u; u < 4u; ++u)
-      X[u] = xp[u][j];
-#pragma unroll
-    for (unsigned u = 0u; u < 4u; ++u)
-#pragma unroll
-      for (unsigned v = 0u; v < 4u; ++v)
-        acc[u][v] = __fma_rn(W[(j + u) & 3u][v], X[u], acc[u][v]);
+    const double X0 = xp0[j], X1 = xp1[j];
+    acc[0][0] = __fma_rn(W[j & 1u][0], X0, acc[0][0]);
+    acc[0][1] = __fma_rn(W[j & 1u][1], X0, acc[0][1]);
+    acc[1][0] = __fma_rn(W[(j + 1u) & 1u][0], X1, acc[1][0]);
+    acc[1][1] = __fma_rn(W[(j + 1u) & 1u][1], X1, acc[1][1]);
     if (j < 63u) {
-#pragma unroll
-      for (unsigned v = 0u; v < 4u; ++v)
-        W[j & 3u][v] = yp[v][j + 4u];
+      W[j & 1u][0] = yp0[j + 2u];
+      W[j & 1u][1] = yp1[j + 2u];
     }
   }
 }
 
-// ---------------------------------------------------------------------------
-// Cholesky of the lower triangle held in R, by one warp: lane x keeps row x.
-// Afterwards R = L^T with zeros below the diagonal.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void chol32_warp(double *const R, const unsigned x)
+// The 136 2x2 tiles of the lower triangle, by x-block xb (16) and y-block
+// yb <= xb.  Group g (0..7) = x-blocks {15 - g, g}: 17 tiles.  A cluster of
+// NSPLIT CTAs deals the groups out: CTA r, Gram warp w takes group
+// r * 4 + w (NSPLIT 2, warps 0..3) or group w (NSPLIT 1, warps 0..7).
+__device__ __forceinline__ bool gram_tile_of(const unsigned group, const unsigned lane, unsigned &x0,
+                                             unsigned &y0)
 {
-  double a[32];
-#pragma unroll
-  for (unsigned j = 0u; j < 32u; ++j)
-    a[j] = (j <= x) ? E32(R, x, j) : 0.0;
-#pragma unroll
-  for (unsigned k = 0u; k < 32u; ++k) {
-    const double akk = __shfl_sync(0xffffffffu, a[k], k);
-    const double rs = rsqrt_rn(akk);
-    const double sq = __dsqrt_rn(akk);
-    if (x > k)
-      a[k] = a[k] * rs;
-    else if (x == k)
-      a[k] = sq;
-#pragma unroll
-    for (unsigned j = k + 1u; j < 32u; ++j) {
-      const double ajk = __shfl_sync(0xffffffffu, a[k], j);
-      if (x >= j)
-        a[j] = __fma_rn(-a[k], ajk, a[j]);
-    }
+  const unsigned xa = 15u - group, xs = group;
+  if (lane <= xa) {
+    x0 = 2u * xa;
+    y0 = 2u * lane;
+    return true;
   }
-  __syncwarp();
-#pragma unroll
-  for (unsigned y = 0u; y < 32u; ++y)
-    E32(R, y, x) = (x >= y) ? a[y] : 0.0;
+  if (lane <= xa + 1u + xs) {
+    x0 = 2u * xs;
+    y0 = 2u * (lane - xa - 1u);
+    return true;
+  }
+  return false;
 }
 
 // ---------------------------------------------------------------------------
-// Inner Jacobi sweep(s).  Warp y owns column pair y of each inner step, lane
-// x row x.  definite != 0: all pairs trigonometric (J = +-I on the block);
-// otherwise columns < npos are +1 and the others -1.
+// Right-looking Cholesky of the lower triangle held in R, by the whole CTA
+// (compact code: it runs once per block pair, from a cold instruction
+// cache).  Column k: warp 0 divides (x > k: times rsqrt_rn(Akk)) and roots
+// the pivot; then the later columns j are updated, spread over the warps,
+// A(x,j) = fma(-A(x,k), A(j,k), A(x,j)) for x >= j.  Afterwards R = L^T
+// with zeros below the diagonal.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void chol32_cta(double *const R, const unsigned tid)
+{
+  const unsigned w = tid >> 5, x = tid & 31u;
+#pragma unroll 1
+  for (unsigned k = 0u; k < 32u; ++k) {
+    if (w == 0u) {
+      const double akk = E32(R, k, k);
+      const double rs = rsqrt_rn(akk);
+      const double sq = __dsqrt_rn(akk);
+      __syncwarp();
+      if (x > k)
+        E32(R, x, k) = E32(R, x, k) * rs;
+      else if (x == k)
+        E32(R, k, k) = sq;
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (unsigned j = k + 1u + w; j < 32u; j += kThreads / 32u)
+      if (x >= j)
+        E32(R, x, j) = __fma_rn(-E32(R, x, k), E32(R, j, k), E32(R, x, j));
+    __syncthreads();
+  }
+  double v[4];
+#pragma unroll
+  for (unsigned i = 0u; i < 4u; ++i) { // element (x = col of R^T, y = row) = (i*256 + tid)
+    const unsigned e = i * kThreads + tid, xx = e >> 5, yy = e & 31u;
+    v[i] = (xx >= yy) ? E32(R, xx, yy) : 0.0;
+  }
+  __syncthreads();
+#pragma unroll
+  for (unsigned i = 0u; i < 4u; ++i) {
+    const unsigned e = i * kThreads + tid, xx = e >> 5, yy = e & 31u;
+    E32(R, yy, xx) = v[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Inner Jacobi sweep(s) on R (32x32) accumulating V_loc, three phases per
+// inner step (16 disjoint column pairs):
+//   A. dot products: warp w, pairs w and w + 8, lane x = row x; Dp, Dq, Apq
+//      by the reference's butterfly (sum32) -> smem;
+//   B. rotations: warp 0, lane y = pair y: relative test, trigonometric or
+//      hyperbolic rotation, sorting decision -> smem (one warp instead of
+//      sixteen computing the same scalars);
+//   C. application: warp w, pairs w and w + 8, lane x = row x.
+// Every operation is the reference's (share/device_code_nosort.hpp:4-222,
+// share/device_code_cdsort.hpp:25-167, share/device_code_cdsort_KISS.hpp).
+// ---------------------------------------------------------------------------
+// Phase A: lane x stores its three products of pair y (row stride 33 keeps
+// the 16 lanes of phase B on distinct banks).
+constexpr unsigned kProdLd = 33u;
+__device__ __forceinline__ void inner_products(const double *const R, const unsigned p, const unsigned q,
+                                               const unsigned x, double *const prod)
+{
+  const double Gp = E32(R, x, p), Gq = E32(R, x, q);
+  prod[0u * kProdLd + x] = __fma_rn(Gp, Gp, 0.0);
+  prod[1u * kProdLd + x] = __fma_rn(Gq, Gq, 0.0);
+  prod[2u * kProdLd + x] = __fma_rn(Gp, Gq, 0.0);
+}
+
+// The 32-lane butterfly of share/device_code_common_Kepler.hpp:26-74 (lane
+// i adds lane i^16, ^8, ^4, ^2, ^1; lane 0's result) evaluated by one thread:
+// the same additions in the same order.
+__device__ __forceinline__ double tree32(const double *const v)
+{
+  double t[16];
+#pragma unroll
+  for (unsigned i = 0u; i < 16u; ++i)
+    t[i] = v[i] + v[i + 16u];
+#pragma unroll
+  for (unsigned k = 8u; k; k >>= 1u)
+#pragma unroll
+    for (unsigned i = 0u; i < k; ++i)
+      t[i] = t[i] + t[i + k];
+  return t[0];
+}
+
+template <bool SORT>
+__device__ __forceinline__ Rot inner_rot(const double Dp, const double Dq, const double Apq, const unsigned p,
+                                         const unsigned q, const int definite, const unsigned npos, unsigned &ts_out,
+                                         unsigned &tb_out)
+{
+  Rot r;
+  r.c = 1.0;
+  r.t = 0.0;
+  r.t_ = 0.0;
+  r.mode = 0;
+  r.scale = 0;
+  r.swap = 0;
+  const double Dp_ = __dsqrt_rn(Dp), Dq_ = __dsqrt_rn(Dq), Apq_ = fabs(Apq), Dpq_ = Dp_ * Dq_;
+  const int ts = !(Apq_ < (Dpq_ * kMyTol));
+  int tb = 0;
+  if (!SORT) {
+    // the rotation is computed whether or not it is applied (no side
+    // effects), so that its latency overlaps the relative test
+    const bool trig = definite || ((p < npos) && (q < npos)) || ((p >= npos) && (q >= npos));
+    double c, t;
+    const int b = trig ? rotT(Apq, Dp, Dq, c, t) : rotH(Apq, Dp, Dq, c, t);
+    if (ts) {
+      r.c = c;
+      r.t = t;
+      r.t_ = trig ? -t : t;
+      tb = b;
+      r.mode = 1;
+      r.scale = tb;
+    }
+  }
+  else {
+    int def;
+    if (definite)
+      def = definite;
+    else if ((p < npos) && (q < npos))
+      def = +1;
+    else if ((p >= npos) && (q >= npos))
+      def = -1;
+    else
+      def = 0;
+    double c, t;
+    const int b = def ? rotT(Apq, Dp, Dq, c, t) : rotH(Apq, Dp, Dq, c, t);
+    if (ts) {
+      double Dp2 = Dp, Dq2 = Dq;
+      r.c = c;
+      r.t = t;
+      tb = b;
+      if (def) {
+        r.t_ = -t;
+        Dp2 = __fma_rn(t, Apq, Dp);
+        Dq2 = __fma_rn(r.t_, Apq, Dq);
+      }
+      else
+        r.t_ = t;
+      r.mode = 1;
+      r.scale = tb;
+      r.swap = !((!def) || ((def > 0) && (Dp2 >= Dq2)) || ((def < 0) && (Dp2 <= Dq2)));
+    }
+    else if (((def > 0) && (Dp < Dq)) || ((def < 0) && (Dq < Dp)))
+      r.mode = 2;
+  }
+  ts_out = (unsigned)ts;
+  tb_out = (unsigned)tb;
+  return r;
+}
+
+__device__ __forceinline__ void inner_apply(double *const R, double *const Vl, const unsigned p, const unsigned q,
+                                            const Rot &r, const unsigned x)
+{
+  if (r.mode == 0)
+    return;
+  const double Gp = E32(R, x, p), Gq = E32(R, x, q);
+  const double Vp = E32(Vl, x, p), Vq = E32(Vl, x, q);
+  if (r.mode == 2) {
+    E32(R, x, p) = Gq;
+    E32(R, x, q) = Gp;
+    E32(Vl, x, p) = Vq;
+    E32(Vl, x, q) = Vp;
+    return;
+  }
+  double np = __fma_rn(r.t_, Gq, Gp), nq = __fma_rn(r.t, Gp, Gq);
+  double vp = __fma_rn(r.t_, Vq, Vp), vq = __fma_rn(r.t, Vp, Vq);
+  if (r.scale) {
+    np = r.c * np;
+    nq = r.c * nq;
+    vp = r.c * vp;
+    vq = r.c * vq;
+  }
+  const unsigned dp = r.swap ? q : p, dq = r.swap ? p : q;
+  E32(R, x, dp) = np;
+  E32(R, x, dq) = nq;
+  E32(Vl, x, dp) = vp;
+  E32(Vl, x, dq) = vq;
+}
+
 template <bool SORT>
 __device__ __forceinline__ void inner_sweeps(double *const R, double *const Vl, const uint8_t *const s0,
                                              const unsigned s0steps, const unsigned nswp, const int definite,
-                                             const unsigned npos, unsigned *const red, const unsigned x,
-                                             const unsigned y, unsigned &blk_s, unsigned &blk_b)
+                                             const unsigned npos, double *const prod, Rot *const rots,
+                                             unsigned *const red, const unsigned x, const unsigned w,
+                                             unsigned &blk_s, unsigned &blk_b)
 {
   blk_s = 0u;
   blk_b = 0u;
   for (unsigned swp = 0u; swp < nswp; ++swp) {
-    unsigned ws = 0u, wb = 0u;
+    unsigned ws = 0u, wb = 0u; // lane y of warp 0: pair y's counts
     for (unsigned step = 0u; step < s0steps; ++step) {
-      const unsigned p = s0[(step * 16u + y) * 2u + 0u];
-      const unsigned q = s0[(step * 16u + y) * 2u + 1u];
-      const double Gp = E32(R, x, p), Gq = E32(R, x, q);
-      const double Vp = E32(Vl, x, p), Vq = E32(Vl, x, q);
-      const double Dp = sum32(__fma_rn(Gp, Gp, 0.0));
-      const double Dq = sum32(__fma_rn(Gq, Gq, 0.0));
-      const double Apq = sum32(__fma_rn(Gp, Gq, 0.0));
-      const double Dp_ = __dsqrt_rn(Dp), Dq_ = __dsqrt_rn(Dq), Apq_ = fabs(Apq), Dpq_ = Dp_ * Dq_;
-      const int ts = !(Apq_ < (Dpq_ * kMyTol));
-      int tb = 0;
-      if (!SORT) {
-        if (ts) {
-          const bool trig = definite || ((p < npos) && (q < npos)) || ((p >= npos) && (q >= npos));
-          double c, t, t_;
-          if (trig) {
-            tb = rotT(Apq, Dp, Dq, c, t);
-            t_ = -t;
-          }
-          else {
-            tb = rotH(Apq, Dp, Dq, c, t);
-            t_ = t;
-          }
-          double np = __fma_rn(t_, Gq, Gp), nq = __fma_rn(t, Gp, Gq);
-          double vp = __fma_rn(t_, Vq, Vp), vq = __fma_rn(t, Vp, Vq);
-          if (tb) {
-            np = c * np;
-            nq = c * nq;
-            vp = c * vp;
-            vq = c * vq;
-          }
-          E32(R, x, p) = np;
-          E32(R, x, q) = nq;
-          E32(Vl, x, p) = vp;
-          E32(Vl, x, q) = vq;
-        }
+      const uint8_t *const st = s0 + step * 32u;
+      const unsigned pa = st[2u * w], qa = st[2u * w + 1u], pb = st[2u * w + 16u], qb = st[2u * w + 17u];
+      inner_products(R, pa, qa, x, prod + 3u * kProdLd * w);
+      inner_products(R, pb, qb, x, prod + 3u * kProdLd * (w + 8u));
+      __syncthreads();
+      if (w == 0u && x < 16u) {
+        const double *const pr = prod + 3u * kProdLd * x;
+        const double Dp = tree32(pr), Dq = tree32(pr + kProdLd), Apq = tree32(pr + 2u * kProdLd);
+        unsigned a, b;
+        rots[x] = inner_rot<SORT>(Dp, Dq, Apq, st[2u * x], st[2u * x + 1u], definite, npos, a, b);
+        ws += a;
+        wb += b;
       }
-      else {
-        int def;
-        if (definite)
-          def = definite;
-        else if ((p < npos) && (q < npos))
-          def = +1;
-        else if ((p >= npos) && (q >= npos))
-          def = -1;
-        else
-          def = 0;
-        if (ts) {
-          double c, t, t_, Dp2 = Dp, Dq2 = Dq;
-          if (def) {
-            tb = rotT(Apq, Dp, Dq, c, t);
-            t_ = -t;
-            Dp2 = __fma_rn(t, Apq, Dp);
-            Dq2 = __fma_rn(t_, Apq, Dq);
-          }
-          else {
-            tb = rotH(Apq, Dp, Dq, c, t);
-            t_ = t;
-          }
-          double np = __fma_rn(t_, Gq, Gp), nq = __fma_rn(t, Gp, Gq);
-          double vp = __fma_rn(t_, Vq, Vp), vq = __fma_rn(t, Vp, Vq);
-          if (tb) {
-            np = c * np;
-            nq = c * nq;
-            vp = c * vp;
-            vq = c * vq;
-          }
-          const bool keep = (!def) || ((def > 0) && (Dp2 >= Dq2)) || ((def < 0) && (Dp2 <= Dq2));
-          const unsigned dp = keep ? p : q, dq = keep ? q : p;
-          E32(R, x, dp) = np;
-          E32(R, x, dq) = nq;
-          E32(Vl, x, dp) = vp;
-          E32(Vl, x, dq) = vq;
-        }
-        else if (((def > 0) && (Dp < Dq)) || ((def < 0) && (Dq < Dp))) {
-          E32(R, x, p) = Gq;
-          E32(R, x, q) = Gp;
-          E32(Vl, x, p) = Vq;
-          E32(Vl, x, q) = Vp;
-        }
-      }
-      ws += (unsigned)ts;
-      wb += (unsigned)tb;
+      __syncthreads();
+      inner_apply(R, Vl, pa, qa, rots[w], x);
+      inner_apply(R, Vl, pb, qb, rots[w + 8u], x);
       __syncthreads();
     }
-    if (x == 0u) {
-      red[y] = ws;
-      red[16u + y] = wb;
+    if (w == 0u) {
+      ws = __reduce_add_sync(0xffffffffu, ws);
+      wb = __reduce_add_sync(0xffffffffu, wb);
+      if (x == 0u) {
+        red[0] = ws;
+        red[1] = wb;
+      }
     }
     __syncthreads();
-    unsigned tot_s = 0u, tot_b = 0u;
-#pragma unroll
-    for (unsigned i = 0u; i < 16u; ++i) {
-      tot_s += red[i];
-      tot_b += red[16u + i];
-    }
+    const unsigned tot_s = red[0], tot_b = red[1];
     __syncthreads();
     if (tot_s) {
       blk_s += tot_s;
@@ -293,8 +412,8 @@ __device__ __forceinline__ void update_stage(const double *const st, const doubl
 // ---------------------------------------------------------------------------
 // The block-pair step kernel.
 // ---------------------------------------------------------------------------
-template <bool SORT, bool ACCV>
-__global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const StepParams P)
+template <bool SORT, bool ACCV, unsigned NSPLIT>
+__global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_constant__ StepParams P)
 {
   extern __shared__ __align__(128) double sm[];
   double *const stg = sm;
@@ -303,9 +422,13 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const StepParams P
   uint8_t *const s0 = reinterpret_cast<uint8_t *>(sm + kOffS0);
   unsigned *const red = reinterpret_cast<unsigned *>(sm + kOffRed);
   uint64_t *const bars = reinterpret_cast<uint64_t *>(sm + kOffBar);
+  double *const prod = sm + kOffProd;
+  Rot *const rots = reinterpret_cast<Rot *>(sm + kOffRots);
 
   const unsigned tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
-  const size_t pidx = ((size_t)P.step * P.pairs + blockIdx.x) * 2u;
+  const unsigned rank = (NSPLIT > 1u) ? (blockIdx.x % NSPLIT) : 0u;
+  const unsigned pair = blockIdx.x / NSPLIT;
+  const size_t pidx = ((size_t)P.step * P.pairs + pair) * 2u;
   const unsigned iBlk = P.strat1[pidx + 0u], jBlk = P.strat1[pidx + 1u];
   double *const Gi = P.G + (size_t)iBlk * kNColB * P.ldG;
   double *const Gj = P.G + (size_t)jBlk * kNColB * P.ldG;
@@ -314,93 +437,101 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const StepParams P
     reinterpret_cast<uint32_t *>(s0)[i] = reinterpret_cast<const uint32_t *>(P.strat0)[i];
   if (tid == 0u) {
     for (unsigned b = 0u; b < 8u; ++b)
-      mbar_init(&bars[b], 1u);
+      mbar_init(&bars[b], (b < kGramStages) ? ((NSPLIT > 1u) ? kThreads / 2u : kThreads) : 1u);
     mbar_fence_init();
   }
   __syncthreads();
 
   // ------------------------------ 1. Gram --------------------------------
-  const unsigned ntile = P.nrow >> 6;
-  const bool gthr = (warp < 4u) && (lane < 9u);
+  const unsigned ntile = P.nrow >> 6; // 64-row tiles
   unsigned gx0 = 0u, gy0 = 0u;
-  if (gthr) { // 36 tiles of 4x4 covering the lower triangle, (xb, yb <= xb)
-    const unsigned t = lane * 4u + warp;
-    unsigned xb = 0u;
-    while (((xb + 1u) * (xb + 2u)) / 2u <= t)
-      ++xb;
-    gx0 = 4u * xb;
-    gy0 = 4u * (t - (xb * (xb + 1u)) / 2u);
-  }
-  double gacc[4][4];
-#pragma unroll
-  for (unsigned u = 0u; u < 4u; ++u)
-#pragma unroll
-    for (unsigned v = 0u; v < 4u; ++v)
-      gacc[u][v] = +0.0;
+  const unsigned gwarps = 8u / NSPLIT;
+  const bool gthr = (warp < gwarps) && gram_tile_of(rank * gwarps + warp, lane, gx0, gy0);
+  double gacc[2][2] = {{+0.0, +0.0}, {+0.0, +0.0}};
 
-  auto issue_gram = [&](const unsigned T) { // warp 0
-    const unsigned s = T % kGramStages;
-    double *const st = stg + s * kGramStage;
-    if (lane == 0u)
-      mbar_arrive_expect_tx(&bars[s], kGramTxBytes);
-    __syncwarp();
-    const double *const src = ((lane < 16u) ? (Gi + (size_t)lane * P.ldG) : (Gj + (size_t)(lane - 16u) * P.ldG)) +
-                              (size_t)T * 64u;
-    double *const dst = st + gcol_off(lane);
-    bulk_g2s(dst, src, 512u, &bars[s]);
-    bulk_g2s(dst + 64u, src, 256u, &bars[s]);
+  const unsigned ngst = (ntile + kGramTiles - 1u) / kGramTiles; // stages of 2 tiles
+  // all threads: 16-byte cp.async of stage k (each column: per tile 32 chunks
+  // of rows 0..63 and 16 chunks repeating rows 0..31), then one arrival on the
+  // stage's mbarrier when this thread's copies have landed
+  // copy producers: in a 2-CTA cluster the 4 warps that compute no Gram
+  // entries (each thread 2 columns' share), else all 8 warps (1 column each);
+  // a column's 48 chunks per tile are spread over its threads in steps of the
+  // thread count per column, rows 0..63 first, then the repeat of rows 0..31
+  const unsigned nprod = (NSPLIT > 1u) ? kThreads / 2u : kThreads;
+  const bool producer = (NSPLIT > 1u) ? (warp >= 4u) : true;
+  const unsigned ptid = (NSPLIT > 1u) ? (tid - kThreads / 2u) : tid;
+  const unsigned tpc = nprod / 32u;                   // threads per column
+  const unsigned pcol = ptid / tpc, psub = ptid % tpc; // this thread's column and offset
+  const double *const pcolp = (pcol < 16u) ? (Gi + (size_t)pcol * P.ldG) : (Gj + (size_t)(pcol - 16u) * P.ldG);
+  auto issue_gram = [&](const unsigned k) {
+    const unsigned s = k % kGramStages;
+    const unsigned nt = min(kGramTiles, ntile - k * kGramTiles);
+    double *const dcol = stg + s * kGramStage + gcol_off(pcol);
+    for (unsigned t = 0u; t < nt; ++t) {
+      const double *const src = pcolp + (size_t)(k * kGramTiles + t) * 64u;
+      for (unsigned q = psub; q < kGramChunks; q += tpc) {
+        const unsigned srow = (q < 32u) ? 2u * q : 2u * q - 64u;
+        cp_async16(dcol + t * 96u + 2u * q, src + srow);
+      }
+    }
+    cp_async_arrive(&bars[s]);
   };
 
-  unsigned issued = 0u;
-  if (warp == 0u)
-    for (; (issued < kGramStages - 1u) && (issued < ntile); ++issued)
-      issue_gram(issued);
-  else
-    issued = (kGramStages - 1u < ntile) ? (kGramStages - 1u) : ntile;
-
-  unsigned T = 0u;
+  if (producer)
+    for (unsigned k = 0u; k + 1u < kGramStages && k < ngst; ++k)
+      issue_gram(k);
+  unsigned k = 0u;
   int failed = 0;
-  for (; T < ntile; ++T) {
-    if (issued < ntile) {
-      if (warp == 0u)
-        issue_gram(issued);
-      ++issued;
-    }
+  for (; k < ngst; ++k) {
+    if (producer && k + kGramStages - 1u < ngst)
+      issue_gram(k + kGramStages - 1u); // into the buffer released at the end of stage k - 1
     int fail = 0;
-    if (warp < 4u) {
-      if (!mbar_wait_bounded(&bars[T % kGramStages], (T / kGramStages) & 1u, kWaitLimit))
+    if (warp < gwarps) {
+      if (!mbar_wait_bounded(&bars[k % kGramStages], (k / kGramStages) & 1u, kWaitLimit))
         fail = 1;
-      else if (gthr)
-        gram_tile(stg + (T % kGramStages) * kGramStage, gx0, gy0, gacc);
+      else if (gthr) {
+        const unsigned nt = min(kGramTiles, ntile - k * kGramTiles);
+        for (unsigned t = 0u; t < nt; ++t)
+          gram_tile(stg + (k % kGramStages) * kGramStage, t * 96u, gx0, gy0, gacc);
+      }
     }
     failed = __syncthreads_or(fail); // uniform decision
     if (failed)
       break;
   }
-  if (failed) { // drain the copies still in flight (bounded), then report
-    if (warp == 0u && lane == 0u) {
-      for (unsigned U = T; U < issued; ++U)
-        (void)mbar_wait_bounded(&bars[U % kGramStages], (U / kGramStages) & 1u, kWaitLimit / 8);
+  if (failed) { // let this thread's copies land before anything else, report
+    cp_async_wait_all();
+    if (tid == 0u)
       atomicOr(P.err, kErrWaitTimeout);
-    }
-    return;
   }
+  // our share of the lower triangle, into our R and the other CTAs' R
   if (gthr) {
 #pragma unroll
-    for (unsigned u = 0u; u < 4u; ++u)
+    for (unsigned u = 0u; u < 2u; ++u)
 #pragma unroll
-      for (unsigned v = 0u; v < 4u; ++v)
-        if (gx0 + u >= gy0 + v)
-          E32(R, gx0 + u, gy0 + v) = gacc[u][v];
+      for (unsigned v = 0u; v < 2u; ++v)
+        if (gx0 + u >= gy0 + v) {
+          const unsigned o = (gy0 + v) * 32u + gx0 + u;
+          R[o] = gacc[u][v];
+          if (NSPLIT > 1u) {
+            cg::cluster_group cl = cg::this_cluster();
+#pragma unroll
+            for (unsigned q = 1u; q < NSPLIT; ++q)
+              cl.map_shared_rank(R, (rank + q) % NSPLIT)[o] = gacc[u][v];
+          }
+        }
   }
-  __syncthreads();
+  if (NSPLIT > 1u)
+    cg::this_cluster().sync(); // release our writes, acquire the others'
+  else
+    __syncthreads();
+  if (failed)
+    return; // the error word is set; the host reports it
 
   // ---------------------------- 2. Cholesky -------------------------------
-  if (warp == 0u)
-    chol32_warp(R, lane);
-  else
-    for (unsigned i = tid - 32u; i < 1024u; i += kThreads - 32u)
-      Vl[i] = ((i >> 5) == (i & 31u)) ? 1.0 : 0.0;
+  for (unsigned i = tid; i < 1024u; i += kThreads)
+    Vl[i] = ((i >> 5) == (i & 31u)) ? 1.0 : 0.0;
+  chol32_cta(R, tid);
   __syncthreads();
 
   // --------------------------- 3. inner sweeps ----------------------------
@@ -434,9 +565,9 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const StepParams P
     }
   }
   unsigned blk_s, blk_b;
-  inner_sweeps<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, lane, warp, blk_s, blk_b);
+  inner_sweeps<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, prod, rots, red, lane, warp, blk_s, blk_b);
 
-  if (tid == 0u && blk_s) {
+  if (rank == 0u && tid == 0u && blk_s) {
     if (blk_b)
       atomicAdd(P.cvg, (((unsigned long long)blk_b) << 32) | blk_s);
     else
@@ -455,10 +586,11 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const StepParams P
   const unsigned nG = (P.nrow + kUpdRows - 1u) / kUpdRows;
   const unsigned nV = ACCV ? (P.ncol + kUpdRows - 1u) / kUpdRows : 0u;
   const unsigned nst = nG + nV;
+  // this CTA's stages: rank, rank + NSPLIT, ...
+  const unsigned nmine = (nst > rank) ? (nst - rank + NSPLIT - 1u) / NSPLIT : 0u;
   double *const Vi = ACCV ? (P.V + (size_t)iBlk * kNColB * P.ldV) : nullptr;
   double *const Vj = ACCV ? (P.V + (size_t)jBlk * kNColB * P.ldV) : nullptr;
 
-  // stage k: rows [base, base + rows) of G (k < nG) or V
   auto stage_geom = [&](const unsigned k, double *&ci, double *&cj, size_t &ld, unsigned &base, unsigned &rows) {
     if (k < nG) {
       ci = Gi;
@@ -475,57 +607,50 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const StepParams P
       rows = min(kUpdRows, P.ncol - base);
     }
   };
-  auto issue_upd = [&](const unsigned k) { // warp 0
-    double *ci, *cj;
-    size_t ld;
-    unsigned base, rows;
-    stage_geom(k, ci, cj, ld, base, rows);
-    const unsigned s = k % kUpdStages, pieces = rows >> 5;
+  auto issue_upd = [&](const unsigned i) { // one thread: this CTA's i-th stage, 2 tensor copies
+    const unsigned k = rank + i * NSPLIT, s = i % kUpdStages;
+    const bool isG = k < nG;
+    const CUtensorMap *const tm = isG ? &P.tmG : &P.tmV;
+    const int piece = (int)(((isG ? k : (k - nG)) * kUpdRows) >> 5);
     double *const st = stg + s * kUpdStage;
-    if (lane == 0u)
-      mbar_arrive_expect_tx(&bars[4u + s], 32u * pieces * 256u);
-    __syncwarp();
-    const double *const src = ((lane < 16u) ? (ci + (size_t)lane * ld) : (cj + (size_t)(lane - 16u) * ld)) + base;
-    double *const dst = st + lane * kUpdColLd;
-    for (unsigned pc = 0u; pc < pieces; ++pc)
-      bulk_g2s(dst + pc * 34u, src + pc * 32u, 256u, &bars[4u + s]);
+    mbar_arrive_expect_tx(&bars[4u + s], 2u * kUpdBoxBytes);
+    tma_load_3d(st, tm, 0, piece, (int)(iBlk * kNColB), &bars[4u + s]);
+    tma_load_3d(st + 16u * kUpdColLd, tm, 0, piece, (int)(jBlk * kNColB), &bars[4u + s]);
   };
 
   __syncthreads(); // VT ready; the Gram stages are free
-  if (warp == 0u)
+  if (tid == 0u && nmine > 0u)
     issue_upd(0u);
-  const unsigned rg = warp, sub = lane & 7u, cg = lane >> 3;
-  for (unsigned k = 0u; k < nst; ++k) {
-    if (warp == 0u && k + 1u < nst)
-      issue_upd(k + 1u);
+  const unsigned rg = warp, sub = lane & 7u, cg8 = lane >> 3;
+  for (unsigned i = 0u; i < nmine; ++i) {
+    if (tid == 0u && i + 1u < nmine)
+      issue_upd(i + 1u);
     int fail = 0;
-    if (warp < 8u) {
-      if (!mbar_wait_bounded(&bars[4u + (k % kUpdStages)], (k / kUpdStages) & 1u, kWaitLimit))
-        fail = 1;
-      else {
-        double *ci, *cj;
-        size_t ld;
-        unsigned base, rows;
-        stage_geom(k, ci, cj, ld, base, rows);
-        if (sub * 32u < rows) {
-          double acc[4][8];
-          update_stage(stg + (k % kUpdStages) * kUpdStage, VT, rg, sub, cg, acc);
-          const unsigned r0 = base + sub * 32u + rg * 4u;
+    if (!mbar_wait_bounded(&bars[4u + (i % kUpdStages)], (i / kUpdStages) & 1u, kWaitLimit))
+      fail = 1;
+    else {
+      double *ci, *cj;
+      size_t ld;
+      unsigned base, rows;
+      stage_geom(rank + i * NSPLIT, ci, cj, ld, base, rows);
+      if (sub * 32u < rows) {
+        double acc[4][8];
+        update_stage(stg + (i % kUpdStages) * kUpdStage, VT, rg, sub, cg8, acc);
+        const unsigned r0 = base + sub * 32u + rg * 4u;
 #pragma unroll
-          for (unsigned v = 0u; v < 8u; ++v) {
-            const unsigned c = cg * 8u + v;
-            double *const col = ((c < 16u) ? (ci + (size_t)c * ld) : (cj + (size_t)(c - 16u) * ld)) + r0;
-            *reinterpret_cast<double2 *>(col) = make_double2(acc[0][v], acc[1][v]);
-            *reinterpret_cast<double2 *>(col + 2u) = make_double2(acc[2][v], acc[3][v]);
-          }
+        for (unsigned v = 0u; v < 8u; ++v) {
+          const unsigned c = cg8 * 8u + v;
+          double *const col = ((c < 16u) ? (ci + (size_t)c * ld) : (cj + (size_t)(c - 16u) * ld)) + r0;
+          *reinterpret_cast<double2 *>(col) = make_double2(acc[0][v], acc[1][v]);
+          *reinterpret_cast<double2 *>(col + 2u) = make_double2(acc[2][v], acc[3][v]);
         }
       }
     }
     if (__syncthreads_or(fail)) { // uniform decision; drain (bounded), report
       if (warp == 0u && lane == 0u) {
-        (void)mbar_wait_bounded(&bars[4u + (k % kUpdStages)], (k / kUpdStages) & 1u, kWaitLimit / 8);
-        if (k + 1u < nst)
-          (void)mbar_wait_bounded(&bars[4u + ((k + 1u) % kUpdStages)], ((k + 1u) / kUpdStages) & 1u,
+        (void)mbar_wait_bounded(&bars[4u + (i % kUpdStages)], (i / kUpdStages) & 1u, kWaitLimit / 8);
+        if (i + 1u < nmine)
+          (void)mbar_wait_bounded(&bars[4u + ((i + 1u) % kUpdStages)], ((i + 1u) / kUpdStages) & 1u,
                                   kWaitLimit / 8);
         atomicOr(P.err, kErrWaitTimeout);
       }
@@ -575,38 +700,85 @@ __global__ void rsqrt_test_kernel(const double *const in, double *const out, con
 }
 
 // ---------------------------------------------------------------------------
-// launchers
+// launchers and tensor maps
 // ---------------------------------------------------------------------------
+cudaError_t make_update_map(CUtensorMap *tm, const double *base, const unsigned nrow, const unsigned ncol,
+                            const unsigned ld)
+{
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess)
+      return e;
+    if (q != cudaDriverEntryPointSuccess || !fn)
+      return cudaErrorNotSupported;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  // (rows within a 32-row piece, pieces, columns); box {34, 8, 16}
+  const cuuint64_t dims[3] = {32u, nrow / 32u, ncol};
+  const cuuint64_t strides[2] = {32u * sizeof(double), (cuuint64_t)ld * sizeof(double)};
+  const cuuint32_t box[3] = {34u, 8u, 16u};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  const CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3u, const_cast<double *>(base), dims, strides, box,
+                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return (r == CUDA_SUCCESS) ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+template <bool S, bool A, unsigned N> static cudaError_t set_smem(const int bytes)
+{
+  return cudaFuncSetAttribute(l1_step_kernel<S, A, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
 cudaError_t l1_configure()
 {
-  const int bytes = (int)l1_smem_bytes();
+  const int b = (int)l1_smem_bytes();
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(l1_step_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)))
+  if ((e = set_smem<false, false, 1u>(b)) || (e = set_smem<false, true, 1u>(b)) || (e = set_smem<true, false, 1u>(b)) ||
+      (e = set_smem<true, true, 1u>(b)) || (e = set_smem<false, false, 2u>(b)) || (e = set_smem<false, true, 2u>(b)) ||
+      (e = set_smem<true, false, 2u>(b)) || (e = set_smem<true, true, 2u>(b)))
     return e;
-  if ((e = cudaFuncSetAttribute(l1_step_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)))
-    return e;
-  if ((e = cudaFuncSetAttribute(l1_step_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)))
-    return e;
-  return cudaFuncSetAttribute(l1_step_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return cudaSuccess;
+}
+
+template <bool S, bool A, unsigned N> static cudaError_t launch(const StepParams &p, cudaStream_t s)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(p.pairs * N);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = l1_smem_bytes();
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = N;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, l1_step_kernel<S, A, N>, p);
+}
+
+unsigned l1_split(const unsigned pairs)
+{
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    (void)cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return (2u * pairs <= (unsigned)sms) ? 2u : 1u;
 }
 
 cudaError_t launch_l1_step(const bool sort, const bool accv, const StepParams &p, cudaStream_t s)
 {
-  const dim3 grid(p.pairs), block(kThreads);
-  const size_t sh = l1_smem_bytes();
-  if (sort) {
-    if (accv)
-      l1_step_kernel<true, true><<<grid, block, sh, s>>>(p);
-    else
-      l1_step_kernel<true, false><<<grid, block, sh, s>>>(p);
+  const unsigned n = p.split;
+  if (n == 2u) {
+    if (sort)
+      return accv ? launch<true, true, 2u>(p, s) : launch<true, false, 2u>(p, s);
+    return accv ? launch<false, true, 2u>(p, s) : launch<false, false, 2u>(p, s);
   }
-  else {
-    if (accv)
-      l1_step_kernel<false, true><<<grid, block, sh, s>>>(p);
-    else
-      l1_step_kernel<false, false><<<grid, block, sh, s>>>(p);
-  }
-  return cudaGetLastError();
+  if (sort)
+    return accv ? launch<true, true, 1u>(p, s) : launch<true, false, 1u>(p, s);
+  return accv ? launch<false, true, 1u>(p, s) : launch<false, false, 1u>(p, s);
 }
 
 cudaError_t launch_initD(double *G, double *D, unsigned nrow, unsigned ncol, unsigned nplus, unsigned ldG,
