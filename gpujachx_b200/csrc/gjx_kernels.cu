@@ -90,52 +90,61 @@ size_t l1_smem_bytes() { return (size_t)kSmemDoubles * sizeof(double); }
 #define E32(A, r, c) (A)[(c) * 32u + (r)]
 
 // ---------------------------------------------------------------------------
-// Gram: one 64-row tile (at row base of the stage) for a 2x2 block of entries
-// (x0+u, y0+v).  Entry (x, y) adds G[r,y]*G[r,x] for r = x, x+1, ..., x+63
-// (mod 64), the reference's order.
+// Gram: one 64-row tile (at row base of the stage) for a 4x2 block of entries
+// (x0+u, y0+v), u < 4, v < 2.  Entry (x, y) adds G[r,y]*G[r,x] for
+// r = x, x+1, ..., x+63 (mod 64), the reference's order.  A window of 4 rows
+// slides down columns y0, y0+1: per row step 4 diagonal operands, 2 new
+// window entries, 8 FMAs.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void gram_tile(const double *const st, const unsigned base, const unsigned x0,
-                                          const unsigned y0, double (&acc)[2][2])
+                                          const unsigned y0, double (&acc)[4][2])
 {
-  const double *const xp0 = st + gcol_off(x0) + base + x0;
-  const double *const xp1 = st + gcol_off(x0 + 1u) + base + x0 + 1u;
+  const double *xp[4];
+#pragma unroll
+  for (unsigned u = 0u; u < 4u; ++u)
+    xp[u] = st + gcol_off(x0 + u) + base + x0 + u;
   const double *const yp0 = st + gcol_off(y0) + base + x0;
   const double *const yp1 = st + gcol_off(y0 + 1u) + base + x0;
-  double W[2][2]; // W[slot][v]: rows x0 + j, x0 + j + 1; slot = row parity
-  W[0][0] = yp0[0];
-  W[0][1] = yp1[0];
-  W[1][0] = yp0[1];
-  W[1][1] = yp1[1];
+  double W[4][2]; // W[slot][v]: rows x0 + j .. x0 + j + 3; slot = row mod 4
+#pragma unroll
+  for (unsigned m = 0u; m < 4u; ++m) {
+    W[m][0] = yp0[m];
+    W[m][1] = yp1[m];
+  }
 #pragma unroll
   for (unsigned j = 0u; j < 64u; ++j) {
-    const double X0 = xp0[j], X1 = xp1[j];
-    acc[0][0] = __fma_rn(W[j & 1u][0], X0, acc[0][0]);
-    acc[0][1] = __fma_rn(W[j & 1u][1], X0, acc[0][1]);
-    acc[1][0] = __fma_rn(W[(j + 1u) & 1u][0], X1, acc[1][0]);
-    acc[1][1] = __fma_rn(W[(j + 1u) & 1u][1], X1, acc[1][1]);
+    double X[4];
+#pragma unroll
+    for (unsigned u = 0u; u < 4u; ++u)
+      X[u] = xp[u][j];
+#pragma unroll
+    for (unsigned u = 0u; u < 4u; ++u) {
+      acc[u][0] = __fma_rn(W[(j + u) & 3u][0], X[u], acc[u][0]);
+      acc[u][1] = __fma_rn(W[(j + u) & 3u][1], X[u], acc[u][1]);
+    }
     if (j < 63u) {
-      W[j & 1u][0] = yp0[j + 2u];
-      W[j & 1u][1] = yp1[j + 2u];
+      W[j & 3u][0] = yp0[j + 4u];
+      W[j & 3u][1] = yp1[j + 4u];
     }
   }
 }
 
-// The 136 2x2 tiles of the lower triangle, by x-block xb (16) and y-block
-// yb <= xb.  Group g (0..7) = x-blocks {15 - g, g}: 17 tiles.  A cluster of
-// NSPLIT CTAs deals the groups out: CTA r, Gram warp w takes group
-// r * 4 + w (NSPLIT 2, warps 0..3) or group w (NSPLIT 1, warps 0..7).
+// The 72 4x2 tiles of the lower triangle: x-block xb (8, rows 4xb..4xb+3),
+// y-block yb <= 2xb + 1 (columns 2yb, 2yb+1).  Group g (0..3) = x-blocks
+// {7 - g, g}: 18 tiles, one per lane.  CTA r of a 2-CTA cluster takes
+// groups 2r and 2r+1 (warps 0, 1); a single CTA takes all four (warps 0..3).
 __device__ __forceinline__ bool gram_tile_of(const unsigned group, const unsigned lane, unsigned &x0,
                                              unsigned &y0)
 {
-  const unsigned xa = 15u - group, xs = group;
-  if (lane <= xa) {
-    x0 = 2u * xa;
+  const unsigned xa = 7u - group, xs = group, na = 2u * xa + 2u, ns = 2u * xs + 2u;
+  if (lane < na) {
+    x0 = 4u * xa;
     y0 = 2u * lane;
     return true;
   }
-  if (lane <= xa + 1u + xs) {
-    x0 = 2u * xs;
-    y0 = 2u * (lane - xa - 1u);
+  if (lane < na + ns) {
+    x0 = 4u * xs;
+    y0 = 2u * (lane - na);
     return true;
   }
   return false;
@@ -338,13 +347,18 @@ __device__ __forceinline__ void inner_sweeps(double *const R, double *const Vl, 
       inner_products(R, pa, qa, x, prod + 3u * kProdLd * w);
       inner_products(R, pb, qb, x, prod + 3u * kProdLd * (w + 8u));
       __syncthreads();
-      if (w == 0u && x < 16u) {
-        const double *const pr = prod + 3u * kProdLd * x;
-        const double Dp = tree32(pr), Dq = tree32(pr + kProdLd), Apq = tree32(pr + 2u * kProdLd);
-        unsigned a, b;
-        rots[x] = inner_rot<SORT>(Dp, Dq, Apq, st[2u * x], st[2u * x + 1u], definite, npos, a, b);
-        ws += a;
-        wb += b;
+      if (w == 0u) { // lanes 0-15 sum Dp of pair x, lanes 16-31 Dq of pair x-16; then Apq
+        const unsigned y = x & 15u;
+        const double *const pr = prod + 3u * kProdLd * y;
+        const double Dpq = tree32(pr + (x >> 4) * kProdLd);
+        const double Apq = tree32(pr + 2u * kProdLd);
+        const double Dq = __shfl_down_sync(0xffffffffu, Dpq, 16);
+        if (x < 16u) {
+          unsigned a, b;
+          rots[x] = inner_rot<SORT>(Dpq, Dq, Apq, st[2u * x], st[2u * x + 1u], definite, npos, a, b);
+          ws += a;
+          wb += b;
+        }
       }
       __syncthreads();
       inner_apply(R, Vl, pa, qa, rots[w], x);
@@ -445,9 +459,9 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
   // ------------------------------ 1. Gram --------------------------------
   const unsigned ntile = P.nrow >> 6; // 64-row tiles
   unsigned gx0 = 0u, gy0 = 0u;
-  const unsigned gwarps = 8u / NSPLIT;
+  const unsigned gwarps = 4u / NSPLIT;
   const bool gthr = (warp < gwarps) && gram_tile_of(rank * gwarps + warp, lane, gx0, gy0);
-  double gacc[2][2] = {{+0.0, +0.0}, {+0.0, +0.0}};
+  double gacc[4][2] = {{+0.0, +0.0}, {+0.0, +0.0}, {+0.0, +0.0}, {+0.0, +0.0}};
 
   const unsigned ngst = (ntile + kGramTiles - 1u) / kGramTiles; // stages of 2 tiles
   // all threads: 16-byte cp.async of stage k (each column: per tile 32 chunks
@@ -507,7 +521,7 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
   // our share of the lower triangle, into our R and the other CTAs' R
   if (gthr) {
 #pragma unroll
-    for (unsigned u = 0u; u < 2u; ++u)
+    for (unsigned u = 0u; u < 4u; ++u)
 #pragma unroll
       for (unsigned v = 0u; v < 2u; ++v)
         if (gx0 + u >= gy0 + v) {
@@ -527,6 +541,25 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
     __syncthreads();
   if (failed)
     return; // the error word is set; the host reports it
+
+  // the first update stage of this CTA: its rows do not change before the
+  // update, so the copy overlaps the Cholesky and the inner sweeps
+  const unsigned nG = (P.nrow + kUpdRows - 1u) / kUpdRows;
+  const unsigned nV = ACCV ? (P.ncol + kUpdRows - 1u) / kUpdRows : 0u;
+  const unsigned nst = nG + nV;
+  const unsigned nmine = (nst > rank) ? (nst - rank + NSPLIT - 1u) / NSPLIT : 0u;
+  auto issue_upd = [&](const unsigned i) { // one thread: this CTA's i-th stage, 2 tensor copies
+    const unsigned k = rank + i * NSPLIT, s = i % kUpdStages;
+    const bool isG = k < nG;
+    const CUtensorMap *const tm = isG ? &P.tmG : &P.tmV;
+    const int piece = (int)(((isG ? k : (k - nG)) * kUpdRows) >> 5);
+    double *const st = stg + s * kUpdStage;
+    mbar_arrive_expect_tx(&bars[4u + s], 2u * kUpdBoxBytes);
+    tma_load_3d(st, tm, 0, piece, (int)(iBlk * kNColB), &bars[4u + s]);
+    tma_load_3d(st + 16u * kUpdColLd, tm, 0, piece, (int)(jBlk * kNColB), &bars[4u + s]);
+  };
+  if (tid == 0u && nmine > 0u)
+    issue_upd(0u);
 
   // ---------------------------- 2. Cholesky -------------------------------
   for (unsigned i = tid; i < 1024u; i += kThreads)
@@ -573,8 +606,11 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
     else
       atomicAdd(reinterpret_cast<unsigned *>(P.cvg), blk_s); // low word, as the reference
   }
-  if (!SORT && !blk_s)
-    return; // no rotation: the block pair is unchanged
+  if (!SORT && !blk_s) { // no rotation: the block pair is unchanged
+    if (tid == 0u && nmine > 0u && !mbar_wait_bounded(&bars[4u], 0u, kWaitLimit))
+      atomicOr(P.err, kErrWaitTimeout); // the prefetched copy has landed before we leave
+    return;
+  }
 
   // ------------------------------ 4. update -------------------------------
   double *const VT = R; // R is dead; B^T[s][c] = V_loc[s][c]
@@ -583,11 +619,6 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
     VT[s * kVTLd + c] = E32(Vl, s, c);
   }
 
-  const unsigned nG = (P.nrow + kUpdRows - 1u) / kUpdRows;
-  const unsigned nV = ACCV ? (P.ncol + kUpdRows - 1u) / kUpdRows : 0u;
-  const unsigned nst = nG + nV;
-  // this CTA's stages: rank, rank + NSPLIT, ...
-  const unsigned nmine = (nst > rank) ? (nst - rank + NSPLIT - 1u) / NSPLIT : 0u;
   double *const Vi = ACCV ? (P.V + (size_t)iBlk * kNColB * P.ldV) : nullptr;
   double *const Vj = ACCV ? (P.V + (size_t)jBlk * kNColB * P.ldV) : nullptr;
 
@@ -607,20 +638,7 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
       rows = min(kUpdRows, P.ncol - base);
     }
   };
-  auto issue_upd = [&](const unsigned i) { // one thread: this CTA's i-th stage, 2 tensor copies
-    const unsigned k = rank + i * NSPLIT, s = i % kUpdStages;
-    const bool isG = k < nG;
-    const CUtensorMap *const tm = isG ? &P.tmG : &P.tmV;
-    const int piece = (int)(((isG ? k : (k - nG)) * kUpdRows) >> 5);
-    double *const st = stg + s * kUpdStage;
-    mbar_arrive_expect_tx(&bars[4u + s], 2u * kUpdBoxBytes);
-    tma_load_3d(st, tm, 0, piece, (int)(iBlk * kNColB), &bars[4u + s]);
-    tma_load_3d(st + 16u * kUpdColLd, tm, 0, piece, (int)(jBlk * kNColB), &bars[4u + s]);
-  };
-
-  __syncthreads(); // VT ready; the Gram stages are free
-  if (tid == 0u && nmine > 0u)
-    issue_upd(0u);
+  __syncthreads(); // VT ready
   const unsigned rg = warp, sub = lane & 7u, cg8 = lane >> 3;
   for (unsigned i = 0u; i < nmine; ++i) {
     if (tid == 0u && i + 1u < nmine)
