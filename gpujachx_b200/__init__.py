@@ -27,13 +27,13 @@ LIB_PATH = os.path.join(PKG, "lib", "libgjx.so")
 STRAT_PATH = os.path.join(PKG, "lib", "strat.so")
 
 CDSORT_1, FULL_SVD, ACCUMV_2, BLK_ORI = 1, 2, 4, 8
-ERR_CUDA, ERR_NO_STRAT, ERR_STRAT_ORDER, ERR_DEVICE, ERR_ALIGN = 1, 2, 3, 4, 5
+ERR_CUDA, ERR_NO_STRAT, ERR_STRAT_ORDER, ERR_DEVICE, ERR_ALIGN, ERR_SCRATCH = 1, 2, 3, 4, 5, 6
 STRATEGIES = ("mmstep", "BrentL", "colcyc", "cycloc", "rowcyc", "cycwor")
 
 # exported by libgjx.so, as declared in include/gjx.h
 EXPORTS = ("hypJacL2", "init_strats", "gjx_init_strats", "gjx_strat_info", "gjx_get_strat1",
            "gjx_hypJacL2_dev", "gjx_release_cache", "gjx_set_verbose", "gjx_last_error",
-           "gjx_version", "gjx_rsqrt_rn_dev", "gjx_profile", "gjx_profile_read")
+           "gjx_version", "gjx_rsqrt_rn_dev", "gjx_profile", "gjx_profile_read", "gjx_hypJacL2_noalloc")
 
 
 class GjxError(RuntimeError):
@@ -70,6 +70,8 @@ def lib() -> ctypes.CDLL:
     L.gjx_hypJacL2_dev.argtypes = [u, u, u, u, ctypes.c_void_p, u, ctypes.c_void_p, u, ctypes.c_void_p,
                                    ctypes.c_void_p, pu, pull, pull]
     L.gjx_hypJacL2_dev.restype = i
+    L.gjx_hypJacL2_noalloc.argtypes = L.gjx_hypJacL2_dev.argtypes
+    L.gjx_hypJacL2_noalloc.restype = i
     L.gjx_release_cache.argtypes = []
     L.gjx_release_cache.restype = i
     L.gjx_set_verbose.argtypes = [i]

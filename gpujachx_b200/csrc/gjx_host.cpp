@@ -154,30 +154,26 @@ double secs(const clk::time_point a, const clk::time_point b)
   return std::chrono::duration<double>(b - a).count();
 }
 
-// The outer sweeps on device data; the caller holds g_mtx and has checked
-// the arguments.  The sweep loop of 1/HypJacL2.cu:167-216.
-int run_sweeps(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
-               double *const dG, const unsigned lddG, double *const dV, const unsigned lddV, double *const dD,
-               const cudaStream_t st, unsigned *const glbSwp, unsigned long long *const glb_s,
-               unsigned long long *const glb_b)
+// The outer sweeps on device data, the sweep loop of 1/HypJacL2.cu:167-216.
+// The caller holds g_mtx, has checked the arguments and the tables, has
+// configured the kernels on this device and provides the device-side
+// working memory: the strategy tables d_s0 / d_s1 (uploaded) and two
+// 64-bit words d_cnt (counter, error word), plus a host mirror h_cnt of
+// those two words.  Nothing is allocated here (profiling events aside,
+// with prof).
+int run_sweeps_core(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
+                    double *const dG, const unsigned lddG, double *const dV, const unsigned lddV, double *const dD,
+                    const cudaStream_t st, const uint8_t *const d_s0, const uint16_t *const d_s1,
+                    unsigned long long *const d_cnt, unsigned long long *const h_cnt, const bool prof,
+                    unsigned *const glbSwp, unsigned long long *const glb_s, unsigned long long *const glb_b)
 {
-  if (!g_strat.loaded)
-    return GJX_ERR_NO_STRAT;
-  if (ncol / gjx::kNColB != g_strat.n1)
-    return GJX_ERR_STRAT_ORDER;
-  DevCtx *ctx = nullptr;
-  if (const int r = dev_ctx(ctx))
-    return r;
-  if (const int r = upload_strat(*ctx, st))
-    return r;
-
   const bool cdsort = (routine & GJX_CDSORT_1) != 0u, full = (routine & GJX_FULL_SVD) != 0u,
              blk_ori = (routine & GJX_BLK_ORI) != 0u;
   if (full) {
     GJX_CUDA(gjx::launch_initV(dV, ncol, lddV, st), "initV");
     ++g_prof.launches;
   }
-  if (g_prof.on && g_prof.ev.size() < 2u * g_strat.steps1) {
+  if (prof && g_prof.ev.size() < 2u * g_strat.steps1) {
     const size_t have = g_prof.ev.size();
     g_prof.ev.resize(2u * g_strat.steps1);
     for (size_t i = have; i < g_prof.ev.size(); ++i)
@@ -187,10 +183,10 @@ int run_sweeps(const unsigned routine, const unsigned nrow, const unsigned ncol,
   gjx::StepParams p{};
   p.G = dG;
   p.V = full ? dV : nullptr;
-  p.strat1 = ctx->d_s1;
-  p.strat0 = ctx->d_s0;
-  p.cvg = ctx->d_cnt;
-  p.err = reinterpret_cast<int *>(ctx->d_cnt + 1);
+  p.strat1 = d_s1;
+  p.strat0 = d_s0;
+  p.cvg = d_cnt;
+  p.err = reinterpret_cast<int *>(d_cnt + 1);
   p.ldG = lddG;
   p.ldV = full ? lddV : 0u;
   p.nrow = nrow;
@@ -205,38 +201,38 @@ int run_sweeps(const unsigned routine, const unsigned nrow, const unsigned ncol,
   if (full)
     GJX_CUDA(gjx::make_update_map(&p.tmV, dV, ncol, ncol, lddV), "tensor map of V");
 
-  GJX_CUDA(cudaMemsetAsync(ctx->d_cnt + 1, 0, sizeof(unsigned long long), st), "clear error word");
+  GJX_CUDA(cudaMemsetAsync(d_cnt + 1, 0, sizeof(unsigned long long), st), "clear error word");
   *glb_s = 0ull;
   *glb_b = 0ull;
   unsigned blk_swp = 0u;
   clk::time_point ts = clk::now();
   while (blk_swp < gjx::kNSweep) {
-    GJX_CUDA(cudaMemsetAsync(ctx->d_cnt, 0, sizeof(unsigned long long), st), "clear counter");
+    GJX_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st), "clear counter");
     for (unsigned stp = 0u; stp < g_strat.steps1; ++stp) {
       p.step = stp;
-      if (g_prof.on)
+      if (prof)
         GJX_CUDA(cudaEventRecord(g_prof.ev[2u * stp], st), "cudaEventRecord");
       GJX_CUDA(gjx::launch_l1_step(cdsort, full, p, st), "block-pair step");
-      if (g_prof.on)
+      if (prof)
         GJX_CUDA(cudaEventRecord(g_prof.ev[2u * stp + 1u], st), "cudaEventRecord");
     }
     g_prof.launches += g_strat.steps1;
     g_prof.l1_launches += g_strat.steps1;
     ++blk_swp;
-    GJX_CUDA(cudaMemcpyAsync(ctx->h_cnt, ctx->d_cnt, 2u * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
+    GJX_CUDA(cudaMemcpyAsync(h_cnt, d_cnt, 2u * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
              "read counters");
     GJX_CUDA(cudaStreamSynchronize(st), "sweep");
-    if (g_prof.on)
+    if (prof)
       for (unsigned stp = 0u; stp < g_strat.steps1; ++stp) {
         float ms = 0.0f;
         GJX_CUDA(cudaEventElapsedTime(&ms, g_prof.ev[2u * stp], g_prof.ev[2u * stp + 1u]), "cudaEventElapsedTime");
         g_prof.l1_ms += ms;
       }
-    if ((int)ctx->h_cnt[1]) {
+    if ((int)h_cnt[1]) {
       g_err = "a block-pair kernel timed out waiting for its tile copies";
       return GJX_ERR_DEVICE;
     }
-    const unsigned long long cvg = ctx->h_cnt[0];
+    const unsigned long long cvg = h_cnt[0];
     const unsigned cvg_s = (unsigned)cvg, cvg_b = (unsigned)(cvg >> 32u);
     *glb_s += cvg_s;
     *glb_b += cvg_b;
@@ -255,6 +251,25 @@ int run_sweeps(const unsigned routine, const unsigned nrow, const unsigned ncol,
   ++g_prof.launches;
   GJX_CUDA(cudaStreamSynchronize(st), "initD");
   return 0;
+}
+
+// run_sweeps_core on the per-device context (allocated on first use)
+int run_sweeps(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
+               double *const dG, const unsigned lddG, double *const dV, const unsigned lddV, double *const dD,
+               const cudaStream_t st, unsigned *const glbSwp, unsigned long long *const glb_s,
+               unsigned long long *const glb_b)
+{
+  if (!g_strat.loaded)
+    return GJX_ERR_NO_STRAT;
+  if (ncol / gjx::kNColB != g_strat.n1)
+    return GJX_ERR_STRAT_ORDER;
+  DevCtx *ctx = nullptr;
+  if (const int r = dev_ctx(ctx))
+    return r;
+  if (const int r = upload_strat(*ctx, st))
+    return r;
+  return run_sweeps_core(routine, nrow, ncol, nplus, dG, lddG, dV, lddV, dD, st, ctx->d_s0, ctx->d_s1, ctx->d_cnt,
+                         ctx->h_cnt, g_prof.on, glbSwp, glb_s, glb_b);
 }
 
 // argument checks of 1/HypJacL2.cu:39-77, same codes in the same order
@@ -307,6 +322,84 @@ template <typename T> int ensure(T *&p, size_t &cap, const size_t n, const char 
 }
 
 } // namespace
+
+namespace gjx {
+
+// Layout of caller-provided scratch: [0, 256) the two words, [256, 1280)
+// strat0, [1280, ...) strat1.
+constexpr size_t kScrCnt = 0u, kScrS0 = 256u, kScrS1 = 1280u;
+
+size_t noalloc_scratch_need()
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  return g_strat.loaded ? (kScrS1 + g_strat.s1.size() * sizeof(uint16_t)) : 0u;
+}
+
+int noalloc_sweeps(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
+                   double *const dG, const unsigned lddG, double *const dV, const unsigned lddV, double *const dD,
+                   void *const stream, void *const scratch, const size_t scratch_bytes, const int dev,
+                   unsigned *const glbSwp, unsigned long long *const glb_s, unsigned long long *const glb_b)
+{
+  struct Uploaded {
+    const void *scratch = nullptr;
+    unsigned long long version = ~0ull;
+    bool configured = false;
+  };
+  static std::vector<Uploaded> up; // per device: what the scratch holds
+  std::lock_guard<std::mutex> lk(g_mtx);
+  if (!g_strat.loaded)
+    return GJX_ERR_NO_STRAT;
+  if (ncol / kNColB != g_strat.n1)
+    return GJX_ERR_STRAT_ORDER;
+  const size_t need = kScrS1 + g_strat.s1.size() * sizeof(uint16_t);
+  if (need > scratch_bytes) {
+    g_err = "the outer strategy table needs " + std::to_string(need) + " bytes of scratch, the static scratch holds " +
+            std::to_string(scratch_bytes);
+    return GJX_ERR_SCRATCH;
+  }
+  if ((size_t)dev >= up.size())
+    up.resize((size_t)dev + 1u);
+  Uploaded &u = up[(size_t)dev];
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  unsigned char *const base = static_cast<unsigned char *>(scratch);
+  if (!u.configured) {
+    GJX_CUDA(l1_configure(), "l1_configure");
+    u.configured = true;
+  }
+  if (u.scratch != scratch || u.version != g_strat.version) {
+    GJX_CUDA(cudaMemcpyAsync(base + kScrS0, g_strat.s0.data(), g_strat.s0.size(), cudaMemcpyHostToDevice, st),
+             "upload strat0");
+    GJX_CUDA(cudaMemcpyAsync(base + kScrS1, g_strat.s1.data(), g_strat.s1.size() * sizeof(uint16_t),
+                             cudaMemcpyHostToDevice, st),
+             "upload strat1");
+    GJX_CUDA(cudaStreamSynchronize(st), "upload strategies");
+    u.scratch = scratch;
+    u.version = g_strat.version;
+  }
+  unsigned long long h_cnt[2] = {0ull, 0ull}; // pageable host mirror of the two words
+  return run_sweeps_core(routine, nrow, ncol, nplus, dG, lddG, dV, lddV, dD, st,
+                         reinterpret_cast<const uint8_t *>(base + kScrS0),
+                         reinterpret_cast<const uint16_t *>(base + kScrS1),
+                         reinterpret_cast<unsigned long long *>(base + kScrCnt), h_cnt, false, glbSwp, glb_s, glb_b);
+}
+
+int check_dev_args(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
+                   const double *const dG, const unsigned lddG, const double *const dV, const unsigned lddV,
+                   const double *const dD, const unsigned *const glbSwp, const unsigned long long *const glb_s,
+                   const unsigned long long *const glb_b)
+{
+  if (const int r = check_args(routine, nrow, ncol, nplus, dG, lddG, dV, lddV, dD, glbSwp, glb_s, glb_b))
+    return r;
+  const bool full = (routine & GJX_FULL_SVD) != 0u;
+  if ((reinterpret_cast<uintptr_t>(dG) & 15u) || (lddG & 1u) || (reinterpret_cast<uintptr_t>(dD) & 7u) ||
+      (full && ((reinterpret_cast<uintptr_t>(dV) & 15u) || (lddV & 1u))))
+    return GJX_ERR_ALIGN;
+  return 0;
+}
+
+void set_error(const char *msg) { g_err = msg; }
+
+} // namespace gjx
 
 extern "C" {
 
@@ -435,12 +528,8 @@ int gjx_hypJacL2_dev(const unsigned routine, const unsigned nrow, const unsigned
                      double *const dD, void *const stream, unsigned *const glbSwp,
                      unsigned long long *const glb_s, unsigned long long *const glb_b)
 {
-  if (const int r = check_args(routine, nrow, ncol, nplus, dG, lddG, dV, lddV, dD, glbSwp, glb_s, glb_b))
+  if (const int r = gjx::check_dev_args(routine, nrow, ncol, nplus, dG, lddG, dV, lddV, dD, glbSwp, glb_s, glb_b))
     return r;
-  const bool full = (routine & GJX_FULL_SVD) != 0u;
-  if ((reinterpret_cast<uintptr_t>(dG) & 15u) || (lddG & 1u) || (reinterpret_cast<uintptr_t>(dD) & 7u) ||
-      (full && ((reinterpret_cast<uintptr_t>(dV) & 15u) || (lddV & 1u))))
-    return GJX_ERR_ALIGN;
   std::lock_guard<std::mutex> lk(g_mtx);
   return run_sweeps(routine, nrow, ncol, nplus, dG, lddG, dV, lddV, dD, static_cast<cudaStream_t>(stream), glbSwp,
                     glb_s, glb_b);

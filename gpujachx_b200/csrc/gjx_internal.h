@@ -46,6 +46,16 @@ cudaError_t launch_initD(double *G, double *D, unsigned nrow, unsigned ncol, uns
                          cudaStream_t s);
 cudaError_t launch_initV(double *V, unsigned ncol, unsigned ldV, cudaStream_t s);
 
+// host driver pieces used by the allocation-free entry point (gjx_noalloc.cu)
+size_t noalloc_scratch_need();
+int noalloc_sweeps(unsigned routine, unsigned nrow, unsigned ncol, unsigned nplus, double *dG, unsigned lddG,
+                   double *dV, unsigned lddV, double *dD, void *stream, void *scratch, size_t scratch_bytes, int dev,
+                   unsigned *glbSwp, unsigned long long *glb_s, unsigned long long *glb_b);
+int check_dev_args(unsigned routine, unsigned nrow, unsigned ncol, unsigned nplus, const double *dG, unsigned lddG,
+                   const double *dV, unsigned lddV, const double *dD, const unsigned *glbSwp,
+                   const unsigned long long *glb_s, const unsigned long long *glb_b);
+void set_error(const char *msg);
+
 // exposed for the parity tests of the primitives
 cudaError_t launch_rsqrt_test(const double *in, double *out, unsigned n, cudaStream_t s);
 

@@ -26,6 +26,7 @@ extern "C" {
 #define GJX_ERR_STRAT_ORDER 3 /* ncol / 16 differs from the loaded outer table order */
 #define GJX_ERR_DEVICE 4      /* a kernel reported a bounded wait that timed out */
 #define GJX_ERR_ALIGN 5       /* device pointer or leading dimension misaligned */
+#define GJX_ERR_SCRATCH 6     /* the tables do not fit the static scratch (gjx_hypJacL2_noalloc) */
 
 /*
  * Replaces hypJacL2 of 1/HypJacL2.hpp:6-27 (definition 1/HypJacL2.cu:13-202).
@@ -86,6 +87,26 @@ int gjx_hypJacL2_dev(const unsigned routine, const unsigned nrow, const unsigned
                      double *const dG, const unsigned lddG, double *const dV, const unsigned lddV,
                      double *const dD, void *const stream, unsigned *const glbSwp,
                      unsigned long long *const glb_s, unsigned long long *const glb_b);
+
+/*
+ * gjx_hypJacL2_dev without any device allocation (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc: a process whose device
+ * memory belongs to a caching allocator or pool, a service that reserves its
+ * memory at start-up, a hot path where cudaMalloc/cudaFree (which synchronise
+ * the device) are not allowed.  The library's device working memory -- the
+ * strategy tables and two 64-bit words -- lives in a static 520 KiB device
+ * array held by every GPU that loads the library until the process exits;
+ * the loaded outer table must fit it (n1 <= 512 blocks, ncol <= 8192), else
+ * GJX_ERR_SCRATCH.  The first call on a device takes the array's address
+ * (cudaGetSymbolAddress) with that device current; make it before any stream
+ * capture.  All calls share the array: each clears its counters and rewrites
+ * the tables when they or the device changed; calls that overlap on the GPU
+ * race.  Same arguments, results and other codes as gjx_hypJacL2_dev.
+ */
+int gjx_hypJacL2_noalloc(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
+                         double *const dG, const unsigned lddG, double *const dV, const unsigned lddV,
+                         double *const dD, void *const stream, unsigned *const glbSwp,
+                         unsigned long long *const glb_s, unsigned long long *const glb_b);
 
 /* Frees the device buffers that hypJacL2 keeps between calls on the current
  * device (they are reused by the next call of the same or smaller size). */
