@@ -107,6 +107,21 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def replica_throughput(local_ms: float, steps: int, world: int, device=None) -> tuple:
+    """Whole-job matrices/s of `world` independent replicas that each ran
+    `steps` decompositions in local_ms of device time: the slowest rank's time
+    counts (max over ranks, as torch.distributed MAX), every rank's matrices
+    count.  Returns (value, max_ms).  Works on gloo (CPU tensors) and nccl."""
+    import torch
+    import torch.distributed as dist
+    t = local_ms
+    if world > 1:
+        x = torch.tensor([local_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(x, op=dist.ReduceOp.MAX)
+        t = float(x.item())
+    return world * steps / (t / 1000.0), t
+
+
 def cpu_port_sample(G0: np.ndarray, sweeps: int, min_seconds: float = 10.0):
     """Time the oracle port (all host threads) on the first outer steps of
     the decomposition; scale by steps per sweep and the sweep count."""
@@ -252,12 +267,7 @@ def main():
     prof = g.profile_read()
     g.profile(False)
     clk = clocks.stop()
-    total_ms = sum(times)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = t.item()
-    value = world * args.steps / (total_ms / 1000.0)
+    value, total_ms = replica_throughput(sum(times), args.steps, world, dev)
 
     # roofline of the block-pair kernel
     l1_mean_s = prof["l1_ms"] / max(1, prof["l1_launches"]) / 1000.0
@@ -290,12 +300,8 @@ def main():
         assert ret == 0, g.last_error()
         if k >= args.warmup:
             e2e_times.append(dt)
-    e2e_s = sum(e2e_times)
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = t.item()
-    e2e = {"value": world * args.steps / e2e_s, "unit": "matrices/s", "h2d_bytes_per_step": M * N * 8,
+    e2e_value, _ = replica_throughput(sum(e2e_times) * 1000.0, args.steps, world, dev)
+    e2e = {"value": e2e_value, "unit": "matrices/s", "h2d_bytes_per_step": M * N * 8,
            "d2h_bytes_per_step": M * N * 8 + N * N * 8 + N * 8, "api": "hypJacL2 (host buffers, pinned)"}
 
     line = {"metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": world, "steps": args.steps,

@@ -643,24 +643,35 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
   for (unsigned i = 0u; i < nmine; ++i) {
     if (tid == 0u && i + 1u < nmine)
       issue_upd(i + 1u);
-    int fail = 0;
-    if (!mbar_wait_bounded(&bars[4u + (i % kUpdStages)], (i / kUpdStages) & 1u, kWaitLimit))
-      fail = 1;
-    else {
+    // a warp computes only if all its lanes saw the stage land (the shuffles
+    // below need the whole warp)
+    const int fail = !__all_sync(0xffffffffu, mbar_wait_bounded(&bars[4u + (i % kUpdStages)], (i / kUpdStages) & 1u,
+                                                                kWaitLimit));
+    if (!fail) {
       double *ci, *cj;
       size_t ld;
       unsigned base, rows;
       stage_geom(rank + i * NSPLIT, ci, cj, ld, base, rows);
-      if (sub * 32u < rows) {
-        double acc[4][8];
-        update_stage(stg + (i % kUpdStages) * kUpdStage, VT, rg, sub, cg8, acc);
-        const unsigned r0 = base + sub * 32u + rg * 4u;
+      double acc[4][8]; // the whole warp computes (rows past the end: discarded)
+      update_stage(stg + (i % kUpdStages) * kUpdStage, VT, rg, sub, cg8, acc);
+      // lanes l and l^8 own the same 4 rows of column groups 2h and 2h+1:
+      // they trade halves so that each store instruction fills whole 32-byte
+      // sectors (rows r0..r0+1 from the even lane, r0+2..r0+3 from the odd
+      // one, same column)
+      const bool live = sub * 32u < rows;
+      const unsigned r0 = base + sub * 32u + rg * 4u;
+      const bool even = !(cg8 & 1u);
+      const unsigned ce = (cg8 & ~1u) * 8u, roff = even ? 0u : 2u;
 #pragma unroll
-        for (unsigned v = 0u; v < 8u; ++v) {
-          const unsigned c = cg8 * 8u + v;
-          double *const col = ((c < 16u) ? (ci + (size_t)c * ld) : (cj + (size_t)(c - 16u) * ld)) + r0;
-          *reinterpret_cast<double2 *>(col) = make_double2(acc[0][v], acc[1][v]);
-          *reinterpret_cast<double2 *>(col + 2u) = make_double2(acc[2][v], acc[3][v]);
+      for (unsigned v = 0u; v < 8u; ++v) {
+        const double s0v = even ? acc[2][v] : acc[0][v], s1v = even ? acc[3][v] : acc[1][v];
+        const double r0v = __shfl_xor_sync(0xffffffffu, s0v, 8), r1v = __shfl_xor_sync(0xffffffffu, s1v, 8);
+        if (live) {
+          const unsigned c1 = ce + v, c2 = ce + 8u + v;
+          double *const col1 = ((c1 < 16u) ? (ci + (size_t)c1 * ld) : (cj + (size_t)(c1 - 16u) * ld)) + r0 + roff;
+          double *const col2 = ((c2 < 16u) ? (ci + (size_t)c2 * ld) : (cj + (size_t)(c2 - 16u) * ld)) + r0 + roff;
+          *reinterpret_cast<double2 *>(col1) = even ? make_double2(acc[0][v], acc[1][v]) : make_double2(r0v, r1v);
+          *reinterpret_cast<double2 *>(col2) = even ? make_double2(r0v, r1v) : make_double2(acc[2][v], acc[3][v]);
         }
       }
     }

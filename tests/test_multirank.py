@@ -1,0 +1,52 @@
+"""The N > 1 path of bench.py on CPU: world size 2 over gloo.
+
+bench.py --gpus N runs N independent replicas (the single-matrix SVD has no
+shard boundary); the whole-job value is all ranks' matrices over the slowest
+rank's time (max over ranks).  Here two gloo ranks report different local
+times and both must get the same aggregate.
+"""
+
+import os
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _rank(rank, world, port, q):
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import bench
+    local_ms = [400.0, 1000.0][rank]
+    value, tmax = bench.replica_throughput(local_ms, steps=5, world=world, device="cpu")
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, value, tmax))
+
+
+def test_replicas_aggregate_over_two_gloo_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29500 + (os.getpid() % 2000)
+    ps = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(timeout=120)
+    got = sorted(q.get(timeout=10) for _ in range(2))
+    for p in ps:
+        assert p.exitcode == 0
+    for _, value, tmax in got:
+        assert tmax == 1000.0                      # the slowest rank
+        assert value == pytest.approx(2 * 5 / 1.0)  # 10 matrices in 1 s
+
+
+def test_single_rank_is_local():
+    sys.path.insert(0, ROOT)
+    import bench
+    v, t = bench.replica_throughput(250.0, steps=2, world=1)
+    assert t == 250.0 and v == pytest.approx(8.0)
