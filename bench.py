@@ -65,6 +65,20 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+PROFILE = os.path.join(ROOT, "profiles", "l1_step_kernel_svd4096x2048.md")
+
+
+def _profiled_traffic():
+    """DRAM bytes (read + write) of one block-pair launch of this workload, as
+    recorded from an ncu capture of it; None when no capture is recorded."""
+    import re
+    if not os.path.exists(PROFILE):
+        return None
+    with open(PROFILE) as f:
+        m = re.search(r"traffic per launch \(read \+ write\) \| ([0-9.]+) MB", f.read())
+    return float(m.group(1)) * 1e6 if m else None
+
+
 class Clocks:
     """nvidia-smi sampler for the timed region (SM clock and throttle reasons)."""
 
@@ -275,11 +289,13 @@ def main():
     ach = BYTES_PER_PAIR * PAIRS / l1_mean_s / 1e9
     flops = FLOP_PER_PAIR * PAIRS / l1_mean_s / 1e12
     roof = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-            "traffic": None, "kernel": "gjx::l1_step_kernel<true,true>",
+            "traffic": _profiled_traffic(), "kernel": "gjx::l1_step_kernel<true,true>",
             "peak_kind": f"{peak_kind} HBM copy bandwidth",
             "launch_ms": l1_mean_s * 1000.0, "launches": prof["l1_launches"],
             "algorithmic_bytes_per_launch": BYTES_PER_PAIR * PAIRS,
-            "algorithmic_flop_per_launch": FLOP_PER_PAIR * PAIRS, "fp64_tflops": flops}
+            "algorithmic_flop_per_launch": FLOP_PER_PAIR * PAIRS, "fp64_tflops": flops,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
+                              "workload (cold L2), recorded in profiles/l1_step_kernel_svd4096x2048.md"}
 
     # e2e through the public host API (pinned buffers, H2D + D2H inside)
     pin = torch.empty((N, M), dtype=torch.float64, pin_memory=True).numpy().T  # Fortran view
