@@ -6,26 +6,32 @@
 //
 //   1. Gram matrix of the M x 32 column pair [G_i G_j], lower triangle only
 //      (the Cholesky never reads the upper one).  Each CTA streams the whole
-//      pair through shared memory in 64-row tiles with the TMA engine
-//      (cp.async.bulk + mbarrier, 4 stages) and computes its share of the
-//      528 entries; every entry is one FMA chain in the reference's row
-//      order (share/device_code_common_Cholesky.hpp:4-56), computed in 2x2
-//      register tiles with a sliding row window.  The shares are exchanged
-//      through distributed shared memory, then one cluster barrier.
-//   2. 32x32 Cholesky in one warp, rows in registers, pivots by shuffles
-//      (share/device_code_common_Cholesky.hpp:58-158).
-//   3. Inner Jacobi sweep(s) on R: each warp owns two column pairs of each
-//      inner step, lane x row x; warp-shuffle dot products in the
-//      reference's butterfly order, trigonometric or hyperbolic rotations,
-//      optional KISS sorting (share/device_code_nosort.hpp,
-//      share/device_code_cdsort.hpp, share/device_code_cdsort_KISS.hpp).
-//      Steps 2 and 3 are deterministic, so every CTA of the cluster
-//      computes them itself and holds the same V_loc bit for bit.
+//      pair through shared memory in 64-row tiles (16-byte cp.async into a
+//      bank-skewed layout with the wrap rows repeated, mbarrier completion,
+//      3 stages of 2 tiles) and computes its share of the 528 entries; every
+//      entry is one FMA chain in the reference's row order
+//      (share/device_code_common_Cholesky.hpp:4-56).  A lane holds the 4
+//      chains (x0..x0+3, y) of one column y: the operands of column x0+u are
+//      shared by the warp, column y slides through a 4-row window, and all
+//      operands come as 16-byte row pairs.  The shares are exchanged through
+//      distributed shared memory, then one cluster barrier.
+//   2. 32x32 Cholesky by the CTA, pivots in warp 0, trailing updates over
+//      all warps (share/device_code_common_Cholesky.hpp:58-158).
+//   3. Inner Jacobi sweep(s) on R, three phases per inner step: the 48 dot
+//      products of the 16 pairs into shared memory, one lane per pair sums
+//      them in the reference's butterfly order and computes its rotation,
+//      then the warps apply the rotations to R and V_loc; trigonometric or
+//      hyperbolic rotations, optional KISS sorting
+//      (share/device_code_nosort.hpp, share/device_code_cdsort.hpp,
+//      share/device_code_cdsort_KISS.hpp).  Steps 2 and 3 are deterministic,
+//      so every CTA of the cluster computes them itself and holds the same
+//      V_loc bit for bit.
 //   4. [G_i G_j] <- [G_i G_j] V_loc (and V likewise): 256-row stages brought
-//      in by the TMA engine, the stages dealt out to the CTAs of the
-//      cluster; each output is a 32-FMA chain in the reference's skewed
-//      order (share/device_code_common.hpp:146-185), computed in 4x8
-//      register tiles along anti-diagonals.
+//      in by TMA tensor copies, the stages dealt out to the CTAs of the
+//      cluster (the first one in flight during steps 2 and 3); each output
+//      is a 32-FMA chain in the reference's skewed order
+//      (share/device_code_common.hpp:146-185), computed in 4x8 register
+//      tiles along anti-diagonals, stored as full 32-byte sectors.
 //
 // All arithmetic is in the reference's order, so results are bit-identical.
 #include <cooperative_groups.h>
@@ -46,12 +52,16 @@ constexpr long long kWaitLimit = 2000000000ll; // ~1 s of cycles per wait
 // rows 0..31, so a chain starting at tile row x reads rows x..x+63 without
 // wrapping.  Filled by 16-byte cp.async (the layout needs 16-byte placement
 // freedom: repeated rows and per-column bank offsets), 3 stages in flight.
+// The offset of column c, 2 ((c + c/8) mod 8) doubles, puts the 16-byte row
+// pairs of 8 consecutive columns in 8 different bank groups (the column
+// stride is 0 mod 16 doubles), and keeps apart the two columns x0 + u that
+// a warp with two x-blocks reads at once.
 constexpr unsigned kGramTiles = 2u;
 constexpr unsigned kGramStages = 3u;
 constexpr unsigned kGramColLd = 2u * 96u + 16u;
 constexpr unsigned kGramStage = 32u * kGramColLd; // doubles
 constexpr unsigned kGramChunks = 48u;             // 16-byte chunks per column and tile
-__device__ __forceinline__ unsigned gcol_off(const unsigned c) { return c * kGramColLd + 2u * ((c >> 1) & 7u); }
+__device__ __forceinline__ unsigned gcol_off(const unsigned c) { return c * kGramColLd + 2u * ((c + (c >> 3)) & 7u); }
 
 // Update staging: 256 rows x 32 columns; the 32-row piece p of column c
 // starts at c*272 + p*34 (2 doubles of skew per piece spread the banks).
@@ -90,61 +100,84 @@ size_t l1_smem_bytes() { return (size_t)kSmemDoubles * sizeof(double); }
 #define E32(A, r, c) (A)[(c) * 32u + (r)]
 
 // ---------------------------------------------------------------------------
-// Gram: one 64-row tile (at row base of the stage) for a 4x2 block of entries
-// (x0+u, y0+v), u < 4, v < 2.  Entry (x, y) adds G[r,y]*G[r,x] for
-// r = x, x+1, ..., x+63 (mod 64), the reference's order.  A window of 4 rows
-// slides down columns y0, y0+1: per row step 4 diagonal operands, 2 new
-// window entries, 8 FMAs.
+// Gram: one 64-row tile (at row base of the stage) for the 4 entries
+// (x0+u, y), u < 4, of one lane.  Entry (x, y) adds G[r,y]*G[r,x] for
+// r = x, x+1, ..., x+63 (mod 64), the reference's order.  With k = r - x0
+// (0..66; rows 64..95 of a tile repeat rows 0..31) chain u takes the k in
+// [u, u+63] in increasing order.  Operands come in 16-byte pairs of rows
+// (k, k+1), k even: one pair of column y and one of each column x0+u per
+// two rows; the pairs of k + 4 are in flight while those of k are used.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void gram_tile(const double *const st, const unsigned base, const unsigned x0,
-                                          const unsigned y0, double (&acc)[4][2])
+                                          const unsigned y, double (&acc)[4])
 {
+  const double *const yp = st + gcol_off(y) + base + x0;
   const double *xp[4];
 #pragma unroll
   for (unsigned u = 0u; u < 4u; ++u)
-    xp[u] = st + gcol_off(x0 + u) + base + x0 + u;
-  const double *const yp0 = st + gcol_off(y0) + base + x0;
-  const double *const yp1 = st + gcol_off(y0 + 1u) + base + x0;
-  double W[4][2]; // W[slot][v]: rows x0 + j .. x0 + j + 3; slot = row mod 4
+    xp[u] = st + gcol_off(x0 + u) + base + x0;
+  double2 Yb[3], Xb[3][4];
 #pragma unroll
-  for (unsigned m = 0u; m < 4u; ++m) {
-    W[m][0] = yp0[m];
-    W[m][1] = yp1[m];
-  }
-#pragma unroll
-  for (unsigned j = 0u; j < 64u; ++j) {
-    double X[4];
+  for (unsigned q = 0u; q < 2u; ++q) {
+    Yb[q] = *reinterpret_cast<const double2 *>(yp + 2u * q);
 #pragma unroll
     for (unsigned u = 0u; u < 4u; ++u)
-      X[u] = xp[u][j];
+      Xb[q][u] = *reinterpret_cast<const double2 *>(xp[u] + 2u * q);
+  }
 #pragma unroll
-    for (unsigned u = 0u; u < 4u; ++u) {
-      acc[u][0] = __fma_rn(W[(j + u) & 3u][0], X[u], acc[u][0]);
-      acc[u][1] = __fma_rn(W[(j + u) & 3u][1], X[u], acc[u][1]);
+  for (unsigned kp = 0u; kp < 34u; ++kp) { // pairs k = 2kp, 2kp + 1
+    if (kp + 2u < 34u) {
+      const unsigned q = (kp + 2u) % 3u;
+      Yb[q] = *reinterpret_cast<const double2 *>(yp + 2u * (kp + 2u));
+#pragma unroll
+      for (unsigned u = 0u; u < 4u; ++u)
+        if (2u * (kp + 2u) + 1u >= u && 2u * (kp + 2u) <= u + 63u)
+          Xb[q][u] = *reinterpret_cast<const double2 *>(xp[u] + 2u * (kp + 2u));
     }
-    if (j < 63u) {
-      W[j & 3u][0] = yp0[j + 4u];
-      W[j & 3u][1] = yp1[j + 4u];
+    const unsigned q = kp % 3u;
+#pragma unroll
+    for (unsigned h = 0u; h < 2u; ++h) {
+      const unsigned k = 2u * kp + h;
+      const double yv = h ? Yb[q].y : Yb[q].x;
+#pragma unroll
+      for (unsigned u = 0u; u < 4u; ++u)
+        if (k >= u && k <= u + 63u)
+          acc[u] = __fma_rn(yv, h ? Xb[q][u].y : Xb[q][u].x, acc[u]);
     }
   }
 }
 
-// The 72 4x2 tiles of the lower triangle: x-block xb (8, rows 4xb..4xb+3),
-// y-block yb <= 2xb + 1 (columns 2yb, 2yb+1).  Group g (0..3) = x-blocks
-// {7 - g, g}: 18 tiles, one per lane.  CTA r of a 2-CTA cluster takes
-// groups 2r and 2r+1 (warps 0, 1); a single CTA takes all four (warps 0..3).
-__device__ __forceinline__ bool gram_tile_of(const unsigned group, const unsigned lane, unsigned &x0,
-                                             unsigned &y0)
+// Lanes of the Gram: x-block xb (rows 4xb..4xb+3) has the lanes y = 0..4xb+3
+// (entries with y > x are computed and dropped).  A warp takes a primary
+// x-block p (lanes 0..4p+3) and possibly a secondary one s (the next 4s+4
+// lanes), so that the 4 operands of column x0+u are shared by the warp.
+//   one CTA:  warps 0..4 = (7), (6,0), (5,1), (4,2), (3)
+//   2-CTA cluster, rank 0: (7), (6,0), (1); rank 1: (5), (4,2), (3)
+template <unsigned NSPLIT>
+__device__ __forceinline__ bool gram_lane_of(const unsigned rank, const unsigned warp, const unsigned lane,
+                                             unsigned &x0, unsigned &y)
 {
-  const unsigned xa = 7u - group, xs = group, na = 2u * xa + 2u, ns = 2u * xs + 2u;
-  if (lane < na) {
-    x0 = 4u * xa;
-    y0 = 2u * lane;
+  int p, sb;
+  if (NSPLIT == 1u) { // (7), (6,0), (5,1), (4,2), (3)
+    if (warp >= 5u)
+      return false;
+    p = 7 - (int)warp;
+    sb = (warp >= 1u && warp <= 3u) ? (int)warp - 1 : -1;
+  } else { // rank 0: (7), (6,0), (1); rank 1: (5), (4,2), (3)
+    if (warp >= 3u)
+      return false;
+    p = (rank == 0u) ? ((warp == 2u) ? 1 : 7 - (int)warp) : 5 - (int)warp;
+    sb = (warp == 1u) ? (rank == 0u ? 0 : 2) : -1;
+  }
+  const unsigned np = 4u * (unsigned)p + 4u;
+  if (lane < np) {
+    x0 = 4u * (unsigned)p;
+    y = lane;
     return true;
   }
-  if (lane < na + ns) {
-    x0 = 4u * xs;
-    y0 = 2u * (lane - na);
+  if (sb >= 0 && lane < np + 4u * (unsigned)sb + 4u) {
+    x0 = 4u * (unsigned)sb;
+    y = lane - np;
     return true;
   }
   return false;
@@ -458,10 +491,10 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
 
   // ------------------------------ 1. Gram --------------------------------
   const unsigned ntile = P.nrow >> 6; // 64-row tiles
-  unsigned gx0 = 0u, gy0 = 0u;
-  const unsigned gwarps = 4u / NSPLIT;
-  const bool gthr = (warp < gwarps) && gram_tile_of(rank * gwarps + warp, lane, gx0, gy0);
-  double gacc[4][2] = {{+0.0, +0.0}, {+0.0, +0.0}, {+0.0, +0.0}, {+0.0, +0.0}};
+  unsigned gx0 = 0u, gy = 0u;
+  const unsigned gwarps = (NSPLIT > 1u) ? 3u : 5u;
+  const bool gthr = gram_lane_of<NSPLIT>(rank, warp, lane, gx0, gy);
+  double gacc[4] = {+0.0, +0.0, +0.0, +0.0};
 
   const unsigned ngst = (ntile + kGramTiles - 1u) / kGramTiles; // stages of 2 tiles
   // all threads: 16-byte cp.async of stage k (each column: per tile 32 chunks
@@ -506,7 +539,7 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
       else if (gthr) {
         const unsigned nt = min(kGramTiles, ntile - k * kGramTiles);
         for (unsigned t = 0u; t < nt; ++t)
-          gram_tile(stg + (k % kGramStages) * kGramStage, t * 96u, gx0, gy0, gacc);
+          gram_tile(stg + (k % kGramStages) * kGramStage, t * 96u, gx0, gy, gacc);
       }
     }
     failed = __syncthreads_or(fail); // uniform decision
@@ -522,18 +555,16 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
   if (gthr) {
 #pragma unroll
     for (unsigned u = 0u; u < 4u; ++u)
+      if (gx0 + u >= gy) {
+        const unsigned o = gy * 32u + gx0 + u;
+        R[o] = gacc[u];
+        if (NSPLIT > 1u) {
+          cg::cluster_group cl = cg::this_cluster();
 #pragma unroll
-      for (unsigned v = 0u; v < 2u; ++v)
-        if (gx0 + u >= gy0 + v) {
-          const unsigned o = (gy0 + v) * 32u + gx0 + u;
-          R[o] = gacc[u][v];
-          if (NSPLIT > 1u) {
-            cg::cluster_group cl = cg::this_cluster();
-#pragma unroll
-            for (unsigned q = 1u; q < NSPLIT; ++q)
-              cl.map_shared_rank(R, (rank + q) % NSPLIT)[o] = gacc[u][v];
-          }
+          for (unsigned q = 1u; q < NSPLIT; ++q)
+            cl.map_shared_rank(R, (rank + q) % NSPLIT)[o] = gacc[u];
         }
+      }
   }
   if (NSPLIT > 1u)
     cg::this_cluster().sync(); // release our writes, acquire the others'
