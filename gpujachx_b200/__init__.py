@@ -33,7 +33,8 @@ STRATEGIES = ("mmstep", "BrentL", "colcyc", "cycloc", "rowcyc", "cycwor")
 # exported by libgjx.so, as declared in include/gjx.h
 EXPORTS = ("hypJacL2", "init_strats", "gjx_init_strats", "gjx_strat_info", "gjx_get_strat1",
            "gjx_hypJacL2_dev", "gjx_release_cache", "gjx_set_verbose", "gjx_last_error",
-           "gjx_version", "gjx_rsqrt_rn_dev", "gjx_profile", "gjx_profile_read", "gjx_hypJacL2_noalloc")
+           "gjx_version", "gjx_rsqrt_rn_dev", "gjx_profile", "gjx_profile_read", "gjx_hypJacL2_noalloc",
+           "gjx_validate_pairs", "gjx_validate_strats")
 
 
 class GjxError(RuntimeError):
@@ -86,6 +87,10 @@ def lib() -> ctypes.CDLL:
     L.gjx_profile.restype = None
     L.gjx_profile_read.argtypes = [pull, pull, pd]
     L.gjx_profile_read.restype = None
+    L.gjx_validate_pairs.argtypes = [ctypes.POINTER(ctypes.c_ushort), u, u, pull, pull, pu]
+    L.gjx_validate_pairs.restype = i
+    L.gjx_validate_strats.argtypes = [pull]
+    L.gjx_validate_strats.restype = i
     L.gjx_set_verbose(0)
     _lib = L
     return L
@@ -123,6 +128,29 @@ def strat1_table() -> np.ndarray:
     if got != n:
         raise GjxError(got, "gjx_get_strat1")
     return out.reshape(info["steps1"], info["pairs1"], 2)
+
+
+def validate_pairs(table) -> dict:
+    """Check a pivot-pair table [steps][n/2][2]: entries in range, p != q,
+    each step a perfect matching, every pair {p, q} covered.  Returns
+    dict(code, missing, repeats, bad_step); code 0 = valid."""
+    t = np.ascontiguousarray(table, dtype=np.uint16)
+    if t.ndim != 3 or t.shape[2] != 2:
+        raise ValueError("table must be [steps][n/2][2]")
+    miss, rep, bad = ctypes.c_ulonglong(), ctypes.c_ulonglong(), ctypes.c_uint()
+    code = lib().gjx_validate_pairs(t.ctypes.data_as(ctypes.POINTER(ctypes.c_ushort)), t.shape[0], 2 * t.shape[1],
+                                    ctypes.byref(miss), ctypes.byref(rep), ctypes.byref(bad))
+    return dict(code=code, missing=miss.value, repeats=rep.value, bad_step=bad.value)
+
+
+def validate_loaded() -> dict:
+    """validate_pairs of both loaded tables (inner strat0, outer strat1)."""
+    out = (ctypes.c_ulonglong * 6)()
+    r = lib().gjx_validate_strats(out)
+    if r < 0:
+        raise GjxError(r, "no strategy tables loaded")
+    return dict(code=r, strat0=dict(code=out[0], missing=out[1], repeats=out[2]),
+                strat1=dict(code=out[3], missing=out[4], repeats=out[5]))
 
 
 def profile(enable: bool) -> None:

@@ -7,6 +7,8 @@
                                                    strat/<family>/NNNNN.h headers,
                                                    symbols "<family>%05u")
 * ``build_x1``    -> gpujachx_b200/lib/x1         (the x1 command line)
+* ``build_pp``    -> gpujachx_b200/lib/libgjx_pp.so (accuracy post-processor, host
+                                                   code in x87 extended precision)
 
 The built files are not committed; they travel with the working tree.
 """
@@ -28,6 +30,7 @@ LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libgjx.so")
 STRAT = os.path.join(LIBDIR, "strat.so")
 X1 = os.path.join(LIBDIR, "x1")
+PP = os.path.join(LIBDIR, "libgjx_pp.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
@@ -77,6 +80,18 @@ def build_x1(force: bool = False, verbose: bool = True) -> str:
     return X1
 
 
+def build_pp(force: bool = False, verbose: bool = True) -> str:
+    src = os.path.join(CSRC, "gjx_pp80.c")
+    if not force and not _newer(PP, [src]):
+        return PP
+    os.makedirs(LIBDIR, exist_ok=True)
+    tmp = PP + ".tmp"
+    _run(["gcc", "-O2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-o", tmp, src,
+          "-lm"], verbose)
+    os.replace(tmp, PP)
+    return PP
+
+
 def build_strat(ref_root: str = "/root/reference", force: bool = False, verbose: bool = True) -> str:
     """Compile the reference's strategy-table headers, where they lie, into strat.so.
 
@@ -120,6 +135,7 @@ def build_all(force: bool = False, verbose: bool = True):
     build_lib(force=force, verbose=verbose)
     build_strat(force=False, verbose=verbose)
     build_x1(force=force, verbose=verbose)
+    build_pp(force=force, verbose=verbose)
 
 
 if __name__ == "__main__":

@@ -523,6 +523,83 @@ int gjx_get_strat1(unsigned short *out, unsigned cap)
   return (int)n;
 }
 
+int gjx_validate_pairs(const unsigned short *const tbl, const unsigned steps, const unsigned n,
+                       unsigned long long *const missing, unsigned long long *const repeats,
+                       unsigned *const bad_step)
+{
+  if (missing)
+    *missing = 0ull;
+  if (repeats)
+    *repeats = 0ull;
+  if (bad_step)
+    *bad_step = 0u;
+  if (!tbl || !steps || !n || (n & 1u))
+    return -1;
+  const unsigned h = n / 2u;
+  std::vector<unsigned> seen((size_t)n * n, 0u);
+  std::vector<unsigned> mark(n, ~0u);
+  for (unsigned st = 0u; st < steps; ++st)
+    for (unsigned k = 0u; k < h; ++k) {
+      const unsigned p = tbl[((size_t)st * h + k) * 2u], q = tbl[((size_t)st * h + k) * 2u + 1u];
+      if (p >= n || q >= n || p == q) {
+        if (bad_step)
+          *bad_step = st;
+        return 1;
+      }
+      if (mark[p] == st || mark[q] == st) { // an index twice in one step
+        if (bad_step)
+          *bad_step = st;
+        return 2;
+      }
+      mark[p] = mark[q] = st;
+      ++seen[(size_t)(p < q ? p : q) * n + (p < q ? q : p)];
+    }
+  unsigned long long miss = 0ull, rep = 0ull;
+  for (unsigned p = 0u; p < n; ++p)
+    for (unsigned q = p + 1u; q < n; ++q) {
+      const unsigned c = seen[(size_t)p * n + q];
+      if (!c)
+        ++miss;
+      else
+        rep += c - 1u;
+    }
+  if (missing)
+    *missing = miss;
+  if (repeats)
+    *repeats = rep;
+  return miss ? 3 : 0;
+}
+
+int gjx_validate_strats(unsigned long long *const out)
+{
+  std::vector<unsigned short> t0, t1;
+  unsigned steps0, n0, steps1, n1;
+  {
+    std::lock_guard<std::mutex> lk(g_mtx);
+    if (!g_strat.loaded)
+      return -GJX_ERR_NO_STRAT;
+    steps0 = g_strat.steps0;
+    n0 = g_strat.n0;
+    steps1 = g_strat.steps1;
+    n1 = g_strat.n1;
+    t0.assign(g_strat.s0.begin(), g_strat.s0.begin() + (size_t)steps0 * n0);
+    t1.assign(g_strat.s1.begin(), g_strat.s1.end());
+  }
+  unsigned long long m0, r0, m1, r1;
+  unsigned b0, b1;
+  const int e0 = gjx_validate_pairs(t0.data(), steps0, n0, &m0, &r0, &b0);
+  const int e1 = gjx_validate_pairs(t1.data(), steps1, n1, &m1, &r1, &b1);
+  if (out) {
+    out[0] = (unsigned long long)e0;
+    out[1] = m0;
+    out[2] = r0;
+    out[3] = (unsigned long long)e1;
+    out[4] = m1;
+    out[5] = r1;
+  }
+  return e0 ? e0 : e1;
+}
+
 int gjx_hypJacL2_dev(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
                      double *const dG, const unsigned lddG, double *const dV, const unsigned lddV,
                      double *const dD, void *const stream, unsigned *const glbSwp,

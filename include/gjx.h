@@ -77,6 +77,21 @@ int gjx_strat_info(unsigned *strat0, unsigned *steps0, unsigned *pairs0, unsigne
 int gjx_get_strat1(unsigned short *out, unsigned cap);
 
 /*
+ * Validate a pivot-pair table tbl[steps][n/2][2] (uint16): every entry
+ * below n, p != q, each step a perfect matching of 0..n-1 (no index twice),
+ * and over the table every unordered pair {p, q} at least once.  Returns 0
+ * (valid), 1 (entry out of range or p == q), 2 (an index twice in a step;
+ * *bad_step says which), 3 (pairs missing: *missing), -1 (bad arguments).
+ * *repeats counts pairs seen more than once (mmstep tables repeat n/2).
+ * No counterpart in the reference, which trusts its tables.
+ */
+int gjx_validate_pairs(const unsigned short *tbl, unsigned steps, unsigned n, unsigned long long *missing,
+                       unsigned long long *repeats, unsigned *bad_step);
+/* Both loaded tables: out[6] = {code0, missing0, repeats0, code1, missing1,
+ * repeats1}; returns the first nonzero code, or -GJX_ERR_NO_STRAT. */
+int gjx_validate_strats(unsigned long long *out);
+
+/*
  * hypJacL2 on device-resident data (no host copies, no per-call allocation
  * of the matrices): dG (lddG >= nrow), dV (lddV >= ncol, routine & 2), dD
  * device pointers, 16-byte aligned, lddG and lddV even.  V is set to I here.

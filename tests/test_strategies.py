@@ -68,3 +68,42 @@ def test_strategy_ids(built):
         info = g.strat_info()
         assert info["strat0"] == i and info["strat1"] == i
         assert info["steps0"] == (32 if fam == "mmstep" else 31)
+
+
+def test_validator_accepts_every_shipped_table(built):
+    """gjx_validate_pairs on all tables up to n1 = 1024: perfect matchings,
+    full coverage; repeats only in mmstep (n/2 pairs twice, n steps)."""
+    import re
+    import subprocess
+    import gpujachx_b200 as g
+    from oracle import oracle
+    syms = subprocess.run(["nm", "-D", "--defined-only", built["strat"]], capture_output=True, text=True).stdout.split()
+    names = sorted({s for s in syms if re.fullmatch(r"[A-Za-z]+\d{5}", s)})
+    assert len(names) == 325
+    for nm in names:
+        fam, n = nm[:-5], int(nm[-5:])
+        t = oracle.load_strat(built["strat"], fam, n)
+        r = g.validate_pairs(t)
+        assert r["code"] == 0 and r["missing"] == 0, nm
+        assert r["repeats"] == (n // 2 if fam == "mmstep" else 0), nm
+    g.init_strats(None, "BrentL", 32, "mmstep", 64)
+    v = g.validate_loaded()
+    assert v["code"] == 0 and v["strat1"]["repeats"] == 32
+
+
+def test_validator_rejects_broken_tables(built):
+    import gpujachx_b200 as g
+    from oracle import oracle
+    t = oracle.load_strat(built["strat"], "cycwor", 16).copy()
+    bad = t.copy()
+    bad[3, 2, 1] = bad[3, 2, 0]          # p == q
+    assert g.validate_pairs(bad)["code"] == 1
+    bad = t.copy()
+    bad[5, 1, 0] = bad[5, 0, 0]          # an index twice in step 5
+    r = g.validate_pairs(bad)
+    assert r["code"] == 2 and r["bad_step"] == 5
+    r = g.validate_pairs(t[:-1])         # drop the last step: its 8 pairs are missing
+    assert r["code"] == 3 and r["missing"] == 8
+    bad = t.copy()
+    bad[0, 0, 0] = 16                    # out of range
+    assert g.validate_pairs(bad)["code"] == 1
