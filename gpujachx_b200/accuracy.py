@@ -124,13 +124,24 @@ def pp80(U, D, V=None, nplus: int | None = None, A=None, ipiv=None, lam=None, uu
     return out
 
 
-def report(r: dict) -> str:
-    """pp80-style text: one line per figure computed."""
+def es25(v: float) -> str:
+    """Fortran ES25.17E3: 17 decimals, a 3-digit signed exponent, width 25."""
+    if math.isnan(v) or math.isinf(v):
+        return f"{v:>25}"
+    m, e = f"{v:.17E}".split("E")
+    return f"{m}E{int(e):+04d}".rjust(25)
+
+
+def report(r: dict, nplus_is_n: bool = False) -> str:
+    """pp80-style text (FORMAT(A,' = ',ES25.17E3)): one line per figure
+    computed; the V lines read V^T V - I when J = I, as the reference's."""
     lines = []
     for lab, v in zip(r["labels"], r["nrms"]):
+        if nplus_is_n:
+            lab = lab.replace("V^T J V - J", "V^T V - I").replace("V J V^T - J", "V V^T - I")
         if not math.isnan(v):
-            lines.append(f"{lab:>20} {v:25.17e}")
+            lines.append(f"{lab} = {es25(v)}")
     if "max_abs_err" in r:
-        lines.append(f"{'max abs err':>20} {r['max_abs_err']:25.17e}")
-        lines.append(f"{'max rel err':>20} {r['max_rel_err']:25.17e}")
+        lines.append(f"max abs err = {es25(r['max_abs_err'])}")
+        lines.append(f"max rel err = {es25(r['max_rel_err'])}")
     return "\n".join(lines)

@@ -523,6 +523,24 @@ int gjx_get_strat1(unsigned short *out, unsigned cap)
   return (int)n;
 }
 
+int gjx_configure_device(const int dev)
+{
+  if (dev < 0) {
+    gjx::set_error("negative device index");
+    return -1;
+  }
+  if (cudaSetDevice(dev) != cudaSuccess) {
+    gjx::set_error("cudaSetDevice failed");
+    return -1;
+  }
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) {
+    gjx::set_error("cudaGetDeviceProperties failed");
+    return -1;
+  }
+  return p.major * 10 + p.minor;
+}
+
 int gjx_validate_pairs(const unsigned short *const tbl, const unsigned steps, const unsigned n,
                        unsigned long long *const missing, unsigned long long *const repeats,
                        unsigned *const bad_step)

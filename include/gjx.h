@@ -76,6 +76,28 @@ int gjx_strat_info(unsigned *strat0, unsigned *steps0, unsigned *pairs0, unsigne
  * number of entries copied (<= cap), or < 0. */
 int gjx_get_strat1(unsigned short *out, unsigned cap);
 
+/* Make dev the calling thread's current device; returns its compute
+ * capability as 10 * major + minor (100 for a B200), or -1.  Stands in for
+ * configureGPU (share/cuda_helper.cu:5-54) minus its process-wide device
+ * flags: nothing here uses mapped host memory. */
+int gjx_configure_device(int dev);
+
+/*
+ * HDF5 (own reader/writer, see gpujachx_b200/csrc/h5mini.h; no libhdf5).
+ * gjx_h5_read: dataset at path ("group/name") into out as doubles
+ * (as_float) or ints; dims[<= 8] and *rank receive its shape; out may be
+ * NULL (shape only); cap = capacity of out in elements.  0 or < 0.
+ * gjx_h5_write: nds datasets into group (one level below the root); mode 0
+ * new file, 1 existing file + new group, 2 existing file, group created if
+ * absent and same-shaped datasets overwritten in place.  dims: 8 entries per
+ * dataset (first ranks[i] used, C order); is_float: double, else int32.
+ * The text of an error is in gjx_last_error().
+ */
+int gjx_h5_read(const char *file, const char *path, int as_float, void *out, unsigned long long cap,
+                unsigned long long *dims, int *rank);
+int gjx_h5_write(const char *file, const char *group, int mode, int nds, const char *const *names, const int *ranks,
+                 const unsigned long long *dims, const int *is_float, const void *const *data);
+
 /*
  * Validate a pivot-pair table tbl[steps][n/2][2] (uint16): every entry
  * below n, p != q, each step a perfect matching of 0..n-1 (no index twice),
