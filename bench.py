@@ -42,18 +42,47 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-M, N, ALG, SEED = 4096, 2048, 11, 1001
-N1 = N // 16
-PAIRS = N1 // 2
-STEPS1 = N1 - 1
+# the single-matrix workloads; "c2" (the default) is the headline
+WORKLOADS = {
+    "c1": dict(m=256, n=256, nplus=256, alg=9, seed=1000, gen="svd_synth", kw=dict(smin=1e-8),
+               metric="SVD matrices/s (256x256 FP64, U and D)",
+               workload="plain FP64 SVD 256x256, G = Q1 diag(s) Q2^T, Haar Q1/Q2 seed 1000, s geometric 1..1e-8, "
+                        "NPLUS=N, cycwor/cycwor, ALG 9 (U, D), one step = one decomposition to convergence"),
+    "c2": dict(m=4096, n=2048, nplus=2048, alg=11, seed=1001, gen="gaussian", kw={},
+               metric="SVD matrices/s (4096x2048 FP64, full SVD)",
+               workload="plain FP64 SVD 4096x2048, i.i.d. N(0,1) seed 1001, NPLUS=N, cycwor/cycwor, ALG 11 "
+                        "(U, V, D), one step = one decomposition to convergence"),
+    "c3": dict(m=2048, n=1024, nplus=512, alg=11, seed=1002, gen="graded", kw={},
+               metric="HSVD matrices/s (2048x1024 FP64, J = diag(+I_512, -I_512), full)",
+               workload="hyperbolic SVD 2048x1024, G = B diag(d), B i.i.d. N(0,1), d_j = 10^U(-6,0), seed 1002, "
+                        "NPLUS=512, cycwor/cycwor, ALG 11 (U, V, D), one step = one decomposition to convergence"),
+}
 W = 32
-FLOP_PER_PAIR = 4 * M * W * W + 2 * N * W * W        # Gram + update of G, update of V
-BYTES_PER_PAIR = 768 * M + 512 * N                    # read G twice, write once; V read + write
-METRIC = "SVD matrices/s (4096x2048 FP64, full SVD)"
-CONFIG = {"workload": "plain FP64 SVD 4096x2048, i.i.d. N(0,1) seed 1001, NPLUS=N, cycwor/cycwor, ALG 11 "
-                      "(U, V, D), one step = one decomposition to convergence",
-          "m": M, "n": N, "alg": ALG, "strategies": "cycwor/cycwor",
-          "l2": "flushed between steps (256 MiB write, outside the timed events)"}
+
+
+def _use(name: str) -> None:
+    """Bind the module-level workload constants to WORKLOADS[name]."""
+    global WL, M, N, NPLUS, ALG, SEED, N1, PAIRS, STEPS1, FLOP_PER_PAIR, BYTES_PER_PAIR, METRIC, CONFIG
+    WL = WORKLOADS[name]
+    M, N, NPLUS, ALG, SEED = WL["m"], WL["n"], WL["nplus"], WL["alg"], WL["seed"]
+    N1 = N // 16
+    PAIRS = N1 // 2
+    STEPS1 = N1 - 1
+    full = bool(ALG & 2)
+    FLOP_PER_PAIR = 4 * M * W * W + (2 * N * W * W if full else 0)   # Gram + update of G, update of V
+    BYTES_PER_PAIR = 768 * M + (512 * N if full else 0)               # G read twice, written once; V read + written
+    METRIC = WL["metric"]
+    CONFIG = {"workload": WL["workload"], "name": name, "m": M, "n": N, "nplus": NPLUS, "alg": ALG,
+              "strategies": "cycwor/cycwor",
+              "l2": "flushed between steps (256 MiB write, outside the timed events)"}
+
+
+def _input() -> np.ndarray:
+    from gpujachx_b200 import synth
+    return synth.make(WL["gen"], M, N, SEED, **WL["kw"])
+
+
+_use("c2")
 
 
 def _peaks():
@@ -149,7 +178,7 @@ def cpu_port_sample(G0: np.ndarray, sweeps: int, min_seconds: float = 10.0):
     cores = os.cpu_count() or 1
     done, t0 = 0, time.perf_counter()
     while done < STEPS1 and (time.perf_counter() - t0) < min_seconds:
-        O.outer_step(ALG, Gf, V, N, s0, s1, done, nthreads=cores)
+        O.outer_step(ALG, Gf, V if ALG & 2 else None, NPLUS, s0, s1, done, nthreads=cores)
         done += 1
     dt = time.perf_counter() - t0
     per_matrix = dt / done * STEPS1 * sweeps
@@ -166,12 +195,32 @@ def lapack_baseline(G0: np.ndarray):
             "routine": "DGESVJ JOBA=G JOBU=U JOBV=V (OpenBLAS 0.3.30 via SciPy)", "seconds": dt}
 
 
+def accuracy_figures(G0: np.ndarray, U: np.ndarray, V, D: np.ndarray) -> dict:
+    """pp80's figures of one result: orthogonality of U, J-orthogonality of V,
+    relative error of D against an FP64 reference spectrum -- LAPACK DGESVJ's
+    sigma^2 for an SVD, eigenvalues of R J R^T (G = QR) for an HSVD."""
+    from gpujachx_b200 import accuracy
+    if NPLUS == N:
+        from oracle import lapack
+        lam = lapack.dgesvj(G0, jobv="N", threads=os.cpu_count() or 1)[0] ** 2
+        ref = "LAPACK DGESVJ sigma^2"
+    else:
+        R = np.linalg.qr(G0, mode="r")
+        J = np.r_[np.ones(NPLUS), -np.ones(N - NPLUS)]
+        lam = np.linalg.eigvalsh((R * J) @ R.T)
+        ref = "eigenvalues of R J R^T, G = QR (absolute accuracy only)"
+    r = accuracy.pp80(U, D, V=V, nplus=NPLUS, lam=lam, uut=(M * M * N <= 2 ** 33))
+    out = {lab: v for lab, v in zip(r["labels"], r["nrms"]) if v == v}
+    out.update(max_rel_err_D=r["max_rel_err"], max_abs_err_D=r["max_abs_err"], reference_spectrum=ref)
+    return out
+
+
 def ref_gpu_once(G0: np.ndarray):
     """The reference's own hypJacL2 built for sm_100a (oracle/_ref), one run."""
     from tests.golden.make_golden import HARNESS, case, run_ref
     if not os.path.exists(HARNESS["base"]):
         return None
-    c = case("bench", M, N, N, ALG, seed=SEED)
+    c = case("bench", M, N, NPLUS, ALG, seed=SEED)
     out = run_ref(c, G0)
     t = out["timing"]
     return {"s_per_matrix_wall": t[0], "s_per_matrix_compute": t[2], "sweeps": out["sweeps"],
@@ -182,8 +231,8 @@ def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from gpujachx_b200 import synth
-    G0 = synth.gaussian(M, N, SEED)
+    _use(args.config)
+    G0 = _input()
     sweeps = int(os.environ.get("GJX_BENCH_SWEEPS", "0"))
     ref = None
     try:
@@ -221,7 +270,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baselines")
+    ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS), help="workload (default: the headline c2)")
+    ap.add_argument("--accuracy", action="store_true", help="add pp80 figures of the last decomposition")
     args = ap.parse_args()
+    _use(args.config)
     if args.impl == "reference":
         return reference_arm(args)
 
@@ -243,7 +295,7 @@ def main():
             dist.barrier()
 
     g.init_strats(None, "cycwor", 32, "cycwor", N1)
-    G0 = synth.gaussian(M, N, SEED)
+    G0 = _input()
     dev = torch.device("cuda", local)
     # device layout: row j of the (N, M) tensor = column j of G
     G0d = torch.tensor(np.ascontiguousarray(G0.T), dtype=torch.float64, device=dev)
@@ -255,7 +307,7 @@ def main():
 
     def step():
         dG.copy_(G0d)
-        ret, swp, s, b = g.hypJacL2_dev(ALG, dG, N, dV, dD, stream=None)
+        ret, swp, s, b = g.hypJacL2_dev(ALG, dG, NPLUS, dV, dD, stream=None)
         return swp
 
     for _ in range(args.warmup):
@@ -289,7 +341,9 @@ def main():
     ach = BYTES_PER_PAIR * PAIRS / l1_mean_s / 1e9
     flops = FLOP_PER_PAIR * PAIRS / l1_mean_s / 1e12
     roof = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-            "traffic": _profiled_traffic(), "kernel": "gjx::l1_step_kernel<true,true>",
+            "traffic": _profiled_traffic() if args.config == "c2" else None,
+            "kernel": "gjx::l1_step_kernel<%s,%s,%d>" % ("true" if ALG & 1 else "false", "true" if ALG & 2 else "false",
+                                                      2 if 2 * PAIRS <= 148 else 1),
             "peak_kind": f"{peak_kind} HBM copy bandwidth",
             "launch_ms": l1_mean_s * 1000.0, "launches": prof["l1_launches"],
             "algorithmic_bytes_per_launch": BYTES_PER_PAIR * PAIRS,
@@ -310,15 +364,16 @@ def main():
         sw, rs, rb = ctypes.c_uint(), ctypes.c_ulonglong(), ctypes.c_ulonglong()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ret = L.hypJacL2(ALG, M, N, N, pd(pin), M, pd(pinV), N, pd(pinD), ctypes.byref(sw), ctypes.byref(rs),
-                         ctypes.byref(rb), None)
+        ret = L.hypJacL2(ALG, M, N, NPLUS, pd(pin), M, pd(pinV) if ALG & 2 else None, N if ALG & 2 else 0, pd(pinD),
+                         ctypes.byref(sw), ctypes.byref(rs), ctypes.byref(rb), None)
         dt = time.perf_counter() - t0
         assert ret == 0, g.last_error()
         if k >= args.warmup:
             e2e_times.append(dt)
     e2e_value, _ = replica_throughput(sum(e2e_times) * 1000.0, args.steps, world, dev)
     e2e = {"value": e2e_value, "unit": "matrices/s", "h2d_bytes_per_step": M * N * 8,
-           "d2h_bytes_per_step": M * N * 8 + N * N * 8 + N * 8, "api": "hypJacL2 (host buffers, pinned)"}
+           "d2h_bytes_per_step": M * N * 8 + (N * N * 8 if ALG & 2 else 0) + N * 8,
+           "api": "hypJacL2 (host buffers, pinned)"}
 
     line = {"metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -326,12 +381,16 @@ def main():
             "config": dict(CONFIG, parallelism=("replicas" if world > 1 else "single GPU")),
             "sweeps": sweeps, "e2e": e2e, "roofline": roof, "clocks": clk,
             "gpu_launches": prof["launches"], "step_ms": times}
+    if rank == 0 and args.accuracy:
+        line["accuracy"] = accuracy_figures(G0, dG.cpu().numpy().T, dV.cpu().numpy().T if ALG & 2 else None,
+                                            dD.cpu().numpy())
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_port_sample(G0, sweeps)
-        try:
-            line["lapack_dgesvj"] = lapack_baseline(G0)
-        except Exception as e:  # noqa: BLE001
-            line["lapack_dgesvj"] = {"error": str(e)[:200]}
+        if NPLUS == N:
+            try:
+                line["lapack_dgesvj"] = lapack_baseline(G0)
+            except Exception as e:  # noqa: BLE001
+                line["lapack_dgesvj"] = {"error": str(e)[:200]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
