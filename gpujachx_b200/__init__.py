@@ -18,7 +18,7 @@ from __future__ import annotations
 import ctypes
 import os
 from dataclasses import dataclass
-from typing import Optional
+from typing import NamedTuple, Optional
 
 import numpy as np
 
@@ -34,7 +34,8 @@ STRATEGIES = ("mmstep", "BrentL", "colcyc", "cycloc", "rowcyc", "cycwor")
 EXPORTS = ("hypJacL2", "init_strats", "gjx_init_strats", "gjx_strat_info", "gjx_get_strat1",
            "gjx_hypJacL2_dev", "gjx_release_cache", "gjx_set_verbose", "gjx_last_error",
            "gjx_version", "gjx_rsqrt_rn_dev", "gjx_profile", "gjx_profile_read", "gjx_hypJacL2_noalloc",
-           "gjx_validate_pairs", "gjx_validate_strats")
+           "gjx_validate_pairs", "gjx_validate_strats", "gjx_configure_device", "gjx_h5_read", "gjx_h5_write",
+           "gjx_hypJacL2_batched")
 
 
 class GjxError(RuntimeError):
@@ -91,6 +92,12 @@ def lib() -> ctypes.CDLL:
     L.gjx_validate_pairs.restype = i
     L.gjx_validate_strats.argtypes = [pull]
     L.gjx_validate_strats.restype = i
+    pp = ctypes.POINTER(ctypes.c_void_p)
+    L.gjx_hypJacL2_batched.argtypes = [u, u, pu, pu, pu, pp, pu, pp, pu, pp, ctypes.c_void_p, pu, pull, pull,
+                                       ctypes.POINTER(ctypes.c_int)]
+    L.gjx_hypJacL2_batched.restype = i
+    L.gjx_configure_device.argtypes = [i]
+    L.gjx_configure_device.restype = i
     L.gjx_set_verbose(0)
     _lib = L
     return L
@@ -230,3 +237,38 @@ def hypJacL2_dev(routine: int, G, nplus: int, V=None, D=None, stream=None, nrow:
     if check and ret:
         raise GjxError(ret, last_error() if ret > 0 else "invalid argument")
     return ret, swp.value, s.value, b.value
+
+
+class BatchResult(NamedTuple):
+    ret: int
+    info: list
+    sweeps: list
+    rot_s: list
+    rot_b: list
+
+
+def hypJacL2_batched(routine: int, Gs, nplus, Vs=None, Ds=None, stream=None, nrows=None) -> BatchResult:
+    """The batched form on device-resident torch tensors, in place: matrix b
+    is Gs[b] ((ncol, lddG) row-major, row j = column j, as hypJacL2_dev),
+    Vs[b] ((ncol, lddV), ALG & 2), Ds[b] ((ncol,)).  nplus: a list, or one
+    value for all.  Each matrix gets exactly what hypJacL2_dev gives it."""
+    n = len(Gs)
+    full = bool(routine & FULL_SVD)
+    npl = list(nplus) if hasattr(nplus, "__len__") else [int(nplus)] * n
+    U = ctypes.c_uint * n
+    P = ctypes.c_void_p * n
+    ncol = U(*[g.shape[0] for g in Gs])
+    ldg = U(*[g.shape[1] for g in Gs])
+    nrow = U(*(nrows if nrows is not None else [g.shape[1] for g in Gs]))
+    dg = P(*[g.data_ptr() for g in Gs])
+    dv = P(*[v.data_ptr() for v in Vs]) if full else None
+    ldv = U(*[v.shape[1] for v in Vs]) if full else None
+    dd = P(*[d.data_ptr() for d in Ds])
+    sw, rs, rb = U(), (ctypes.c_ulonglong * n)(), (ctypes.c_ulonglong * n)()
+    info = (ctypes.c_int * n)()
+    st = stream.cuda_stream if stream is not None else None
+    ret = lib().gjx_hypJacL2_batched(routine, n, nrow, ncol, U(*npl), dg, ldg, dv, ldv, dd, st, sw, rs, rb, info)
+    if ret:
+        raise GjxError(ret, last_error())
+    return BatchResult(ret, list(info), list(sw), list(rs), list(rb))
+

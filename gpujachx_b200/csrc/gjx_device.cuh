@@ -168,6 +168,11 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, const uint32_t count)
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 
+__device__ __forceinline__ void mbar_inval(uint64_t *bar)
+{
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"((uint32_t)__cvta_generic_to_shared(bar)) : "memory");
+}
+
 __device__ __forceinline__ void mbar_fence_init()
 {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");

@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <dlfcn.h>
 #include <mutex>
 #include <string>
@@ -39,6 +40,7 @@ struct Strat {
   std::vector<uint8_t> s0;  // [32][16][2], steps0 rows used
   std::vector<uint16_t> s1; // [steps1][pairs1][2]
   unsigned long long version = 0ull;
+  std::string sdy, snp1;    // where other outer tables of the family come from (batched form)
 };
 
 std::mutex g_mtx;
@@ -92,6 +94,12 @@ struct DevCtx {
   unsigned long long version = ~0ull;
   unsigned long long *d_cnt = nullptr; // [0] = cvg, [1] = err (int in the low word)
   unsigned long long *h_cnt = nullptr; // pinned mirror
+  // outer tables of the batched form, by n1, for strategy version btab_version
+  bool batch_ready = false;
+  cudaStream_t batch_stream = nullptr; // graphs cannot be captured on the legacy default stream
+  cudaEvent_t batch_ev = nullptr;
+  std::vector<std::pair<uint16_t *, unsigned>> btab; // index n1: (device table, steps)
+  unsigned long long btab_version = ~0ull;
   // cached matrices of hypJacL2
   double *dG = nullptr, *dV = nullptr, *dD = nullptr;
   size_t capG = 0u, capV = 0u, capD = 0u;
@@ -308,6 +316,247 @@ int check_args(const unsigned routine, const unsigned nrow, const unsigned ncol,
   return 0;
 }
 
+// the outer table of the loaded family for n1 blocks, resident on this
+// device (loaded from the strategy library on first use)
+int batch_table(DevCtx &ctx, const unsigned n1, const uint16_t *&dtab, unsigned &steps)
+{
+  if (ctx.btab_version != g_strat.version) {
+    for (auto &t : ctx.btab)
+      if (t.first)
+        (void)cudaFree(t.first);
+    ctx.btab.clear();
+    ctx.btab_version = g_strat.version;
+  }
+  if (ctx.btab.size() <= n1)
+    ctx.btab.resize(n1 + 1u, {nullptr, 0u});
+  if (!ctx.btab[n1].first) {
+    unsigned st = 0u;
+    if (!strat_id(g_strat.snp1.c_str(), n1, st)) {
+      g_err = "no " + g_strat.snp1 + " table for n1 = " + std::to_string(n1);
+      return GJX_ERR_NO_STRAT;
+    }
+    void *const h = dlopen(g_strat.sdy.c_str(), RTLD_LAZY);
+    if (!h) {
+      g_err = "cannot open " + g_strat.sdy;
+      return GJX_ERR_NO_STRAT;
+    }
+    const void *const a = strat_ptr(h, g_strat.snp1.c_str(), n1);
+    if (!a) {
+      dlclose(h);
+      g_err = "no " + g_strat.snp1 + " table for n1 = " + std::to_string(n1) + " in " + g_strat.sdy;
+      return GJX_ERR_NO_STRAT;
+    }
+    const size_t e = (size_t)st * (n1 / 2u) * 2u;
+    std::vector<uint16_t> t(e);
+    if (n1 <= 256u)
+      for (size_t i = 0u; i < e; ++i)
+        t[i] = static_cast<const uint8_t *>(a)[i];
+    else
+      std::memcpy(t.data(), a, e * sizeof(uint16_t));
+    dlclose(h);
+    uint16_t *d = nullptr;
+    GJX_CUDA(cudaMalloc(&d, e * sizeof(uint16_t)), "cudaMalloc(batch table)");
+    GJX_CUDA(cudaMemcpy(d, t.data(), e * sizeof(uint16_t), cudaMemcpyHostToDevice), "upload batch table");
+    ctx.btab[n1] = {d, st};
+  }
+  dtab = ctx.btab[n1].first;
+  steps = ctx.btab[n1].second;
+  return 0;
+}
+
+// The batched form: nmat independent decompositions, each exactly as
+// run_sweeps_core would do it alone (same steps, same per-pair code, same
+// convergence test), run together: one launch per outer step index for all
+// matrices, the launches of a sweep replayed from a CUDA graph.
+int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const nrow, const unsigned *const ncol,
+              const unsigned *const nplus, double *const *const dG, const unsigned *const lddG,
+              double *const *const dV, const unsigned *const lddV, double *const *const dD, cudaStream_t st,
+              unsigned *const sweeps, unsigned long long *const glb_s, unsigned long long *const glb_b,
+              int *const info)
+{
+  const bool cdsort = (routine & GJX_CDSORT_1) != 0u, full = (routine & GJX_FULL_SVD) != 0u,
+             blk_ori = (routine & GJX_BLK_ORI) != 0u;
+  DevCtx *ctx = nullptr;
+  if (const int r = dev_ctx(ctx))
+    return r;
+  if (!ctx->batch_ready) {
+    GJX_CUDA(gjx::batch_configure(), "batch_configure");
+    GJX_CUDA(cudaStreamCreateWithFlags(&ctx->batch_stream, cudaStreamNonBlocking), "batch stream");
+    GJX_CUDA(cudaEventCreateWithFlags(&ctx->batch_ev, cudaEventDisableTiming), "batch event");
+    ctx->batch_ready = true;
+  }
+  if (!st) { // the legacy stream: work on our own stream, after what the caller queued
+    GJX_CUDA(cudaEventRecord(ctx->batch_ev, nullptr), "batch event");
+    GJX_CUDA(cudaStreamWaitEvent(ctx->batch_stream, ctx->batch_ev, 0u), "batch event");
+    st = ctx->batch_stream;
+  }
+  if (const int r = upload_strat(*ctx, st))
+    return r;
+
+  std::vector<gjx::BatchMat> mats(nmat);
+  std::vector<uint32_t> ok(nmat, 0u);
+  unsigned max_steps = 0u;
+  for (unsigned b = 0u; b < nmat; ++b) {
+    sweeps[b] = 0u;
+    glb_s[b] = glb_b[b] = 0ull;
+    unsigned dummy_s = 0u;
+    unsigned long long dummy_l = 0ull;
+    info[b] = gjx::check_dev_args(routine, nrow[b], ncol[b], nplus[b], dG[b], lddG[b], full ? dV[b] : nullptr,
+                                  full ? lddV[b] : 0u, dD[b], &dummy_s, &dummy_l, &dummy_l);
+    if (info[b])
+      continue;
+    const unsigned n1 = ncol[b] / gjx::kNColB;
+    const uint16_t *tab = nullptr;
+    unsigned steps = 0u;
+    if (const int r = batch_table(*ctx, n1, tab, steps))
+      return r;
+    gjx::StepParams &p = mats[b].p;
+    p.G = dG[b];
+    p.V = full ? dV[b] : nullptr;
+    p.strat1 = tab;
+    p.strat0 = ctx->d_s0;
+    p.ldG = lddG[b];
+    p.ldV = full ? lddV[b] : 0u;
+    p.nrow = nrow[b];
+    p.ncol = ncol[b];
+    p.nplus = nplus[b];
+    p.pairs = n1 / 2u;
+    p.s0steps = g_strat.steps0;
+    p.nswp0 = blk_ori ? 1u : gjx::kNSweep;
+    p.gdefinite = (nplus[b] ? ((nplus[b] < ncol[b]) ? 0 : +1) : -1);
+    p.split = 1u;
+    GJX_CUDA(gjx::make_update_map(&p.tmG, dG[b], nrow[b], ncol[b], lddG[b]), "tensor map of G");
+    if (full)
+      GJX_CUDA(gjx::make_update_map(&p.tmV, dV[b], ncol[b], ncol[b], lddV[b]), "tensor map of V");
+    mats[b].D = dD[b];
+    mats[b].steps1 = steps;
+    ok[b] = 1u;
+    if (steps > max_steps)
+      max_steps = steps;
+  }
+  // the work of each step index: block pairs of the matrices that have it,
+  // the largest matrices first (fewest stragglers at the end of a launch)
+  std::vector<unsigned> order;
+  for (unsigned b = 0u; b < nmat; ++b)
+    if (ok[b])
+      order.push_back(b);
+  std::stable_sort(order.begin(), order.end(), [&](unsigned x, unsigned y) {
+    return (unsigned long long)nrow[x] * ncol[x] > (unsigned long long)nrow[y] * ncol[y];
+  });
+  std::vector<uint32_t> items;
+  std::vector<unsigned> off(max_steps + 1u, 0u);
+  for (unsigned s = 0u; s < max_steps; ++s) {
+    off[s] = (unsigned)items.size();
+    for (unsigned b : order)
+      if (s < mats[b].steps1)
+        for (unsigned q = 0u; q < mats[b].p.pairs; ++q)
+          items.push_back((b << 16u) | q);
+  }
+  off[max_steps] = (unsigned)items.size();
+  if (order.empty())
+    return 0;
+
+  // device memory of the batch, one allocation
+  auto up = [](size_t x) { return (x + 255u) & ~(size_t)255u; };
+  const size_t o_mats = 0u, o_cvg = up(o_mats + nmat * sizeof(gjx::BatchMat)), o_done = up(o_cvg + nmat * 8u),
+               o_ok = up(o_done + nmat * 4u), o_swp = up(o_ok + nmat * 4u), o_gs = up(o_swp + nmat * 4u),
+               o_gb = up(o_gs + nmat * 8u), o_q = up(o_gb + nmat * 8u), o_act = up(o_q + max_steps * 4u),
+               o_err = up(o_act + 4u), o_items = up(o_err + 8u), total = up(o_items + items.size() * 4u);
+  char *mem = nullptr;
+  GJX_CUDA(cudaMalloc(&mem, total), "cudaMalloc(batch)");
+  struct Free {
+    char *m;
+    ~Free() { (void)cudaFree(m); }
+  } free_mem{mem};
+  auto *d_mats = reinterpret_cast<gjx::BatchMat *>(mem + o_mats);
+  auto *d_cvg = reinterpret_cast<unsigned long long *>(mem + o_cvg);
+  auto *d_done = reinterpret_cast<uint32_t *>(mem + o_done);
+  auto *d_ok = reinterpret_cast<uint32_t *>(mem + o_ok);
+  auto *d_swp = reinterpret_cast<unsigned *>(mem + o_swp);
+  auto *d_gs = reinterpret_cast<unsigned long long *>(mem + o_gs);
+  auto *d_gb = reinterpret_cast<unsigned long long *>(mem + o_gb);
+  auto *d_q = reinterpret_cast<unsigned *>(mem + o_q);
+  auto *d_act = reinterpret_cast<unsigned *>(mem + o_act);
+  auto *d_err = reinterpret_cast<int *>(mem + o_err);
+  auto *d_items = reinterpret_cast<uint32_t *>(mem + o_items);
+  for (unsigned b = 0u; b < nmat; ++b) {
+    mats[b].p.cvg = d_cvg + b;
+    mats[b].p.err = d_err;
+  }
+  std::vector<uint32_t> done(nmat);
+  for (unsigned b = 0u; b < nmat; ++b)
+    done[b] = ok[b] ? 0u : 1u;
+  GJX_CUDA(cudaMemsetAsync(mem + o_cvg, 0, o_items - o_cvg, st), "clear batch words");
+  GJX_CUDA(cudaMemcpyAsync(d_mats, mats.data(), nmat * sizeof(gjx::BatchMat), cudaMemcpyHostToDevice, st),
+           "upload batch");
+  GJX_CUDA(cudaMemcpyAsync(d_done, done.data(), nmat * 4u, cudaMemcpyHostToDevice, st), "upload batch");
+  GJX_CUDA(cudaMemcpyAsync(d_ok, ok.data(), nmat * 4u, cudaMemcpyHostToDevice, st), "upload batch");
+  GJX_CUDA(cudaMemcpyAsync(d_items, items.data(), items.size() * 4u, cudaMemcpyHostToDevice, st), "upload batch");
+  if (full) {
+    GJX_CUDA(gjx::launch_batch_initV(d_mats, nmat, st), "batch initV");
+    ++g_prof.launches;
+  }
+
+  int dev = 0, sms = 148;
+  GJX_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  GJX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+
+  // one sweep, captured once
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  GJX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+  cudaError_t ce = cudaSuccess;
+  for (unsigned s = 0u; s < max_steps && ce == cudaSuccess; ++s) {
+    gjx::BatchStep bs{d_mats, d_items + off[s], off[s + 1u] - off[s], s, d_q, d_done, d_err};
+    const unsigned ctas = std::min<unsigned>((unsigned)sms, bs.nitems);
+    ce = gjx::launch_batch_step(cdsort, full, bs, ctas, st);
+  }
+  if (ce == cudaSuccess)
+    ce = cudaMemsetAsync(d_act, 0, 4u, st);
+  gjx::BatchSweep sw{d_cvg, d_done, d_swp, d_gs, d_gb, d_q, d_act, nmat, max_steps};
+  if (ce == cudaSuccess)
+    ce = gjx::launch_batch_sweep_end(sw, st);
+  const cudaError_t ee = cudaStreamEndCapture(st, &graph);
+  GJX_CUDA(ce, "capture of a batch sweep");
+  GJX_CUDA(ee, "end capture");
+  struct Graph {
+    cudaGraph_t g;
+    cudaGraphExec_t *x;
+    ~Graph()
+    {
+      if (*x)
+        (void)cudaGraphExecDestroy(*x);
+      if (g)
+        (void)cudaGraphDestroy(g);
+    }
+  } guard{graph, &exec};
+  GJX_CUDA(cudaGraphInstantiate(&exec, graph, 0ull), "graph instantiate");
+
+  unsigned active = 0u;
+  int err = 0;
+  for (unsigned k = 0u; k < gjx::kNSweep; ++k) {
+    GJX_CUDA(cudaGraphLaunch(exec, st), "graph launch");
+    g_prof.launches += max_steps + 1u;
+    g_prof.l1_launches += max_steps;
+    GJX_CUDA(cudaMemcpyAsync(&active, d_act, 4u, cudaMemcpyDeviceToHost, st), "read batch state");
+    GJX_CUDA(cudaMemcpyAsync(&err, d_err, 4u, cudaMemcpyDeviceToHost, st), "read batch state");
+    GJX_CUDA(cudaStreamSynchronize(st), "batch sweep");
+    if (err) {
+      g_err = "a block-pair kernel timed out waiting for its tile copies";
+      return GJX_ERR_DEVICE;
+    }
+    if (!active)
+      break;
+  }
+  GJX_CUDA(gjx::launch_batch_initD(d_mats, nmat, d_ok, st), "batch initD");
+  ++g_prof.launches;
+  GJX_CUDA(cudaMemcpyAsync(sweeps, d_swp, nmat * 4u, cudaMemcpyDeviceToHost, st), "read sweeps");
+  GJX_CUDA(cudaMemcpyAsync(glb_s, d_gs, nmat * 8u, cudaMemcpyDeviceToHost, st), "read counts");
+  GJX_CUDA(cudaMemcpyAsync(glb_b, d_gb, nmat * 8u, cudaMemcpyDeviceToHost, st), "read counts");
+  GJX_CUDA(cudaStreamSynchronize(st), "batch end");
+  return 0;
+}
+
 template <typename T> int ensure(T *&p, size_t &cap, const size_t n, const char *const what)
 {
   if (n <= cap)
@@ -461,6 +710,8 @@ int gjx_init_strats(const char *const sdy, const char *const snp0, const unsigne
   else
     std::memcpy(s.s1.data(), a1, e1 * sizeof(uint16_t));
   dlclose(h);
+  s.sdy = sdy;
+  s.snp1 = snp1;
   s.loaded = true;
   std::lock_guard<std::mutex> lk(g_mtx);
   s.version = g_strat.version + 1ull;
@@ -738,6 +989,26 @@ int gjx_rsqrt_rn_dev(const double *in, double *out, const unsigned n)
   GJX_CUDA(gjx::launch_rsqrt_test(in, out, n, nullptr), "rsqrt_rn");
   GJX_CUDA(cudaStreamSynchronize(nullptr), "rsqrt_rn");
   return 0;
+}
+
+int gjx_hypJacL2_batched(const unsigned routine, const unsigned nmat, const unsigned *const nrow,
+                         const unsigned *const ncol, const unsigned *const nplus, double *const *const dG,
+                         const unsigned *const lddG, double *const *const dV, const unsigned *const lddV,
+                         double *const *const dD, void *const stream, unsigned *const sweeps,
+                         unsigned long long *const glb_s, unsigned long long *const glb_b, int *const info)
+{
+  if (!nmat || nmat > 65535u || !nrow || !ncol || !nplus || !dG || !lddG || !dD || !sweeps || !glb_s || !glb_b ||
+      !info || ((routine & GJX_FULL_SVD) && (!dV || !lddV)) || routine >= 16u) {
+    g_err = "gjx_hypJacL2_batched: bad arguments";
+    return -1;
+  }
+  std::lock_guard<std::mutex> lk(g_mtx);
+  if (!g_strat.loaded) {
+    g_err = "init_strats has not loaded strategy tables";
+    return GJX_ERR_NO_STRAT;
+  }
+  return run_batch(routine, nmat, nrow, ncol, nplus, dG, lddG, dV, lddV, dD, static_cast<cudaStream_t>(stream),
+                   sweeps, glb_s, glb_b, info);
 }
 
 } // extern "C"

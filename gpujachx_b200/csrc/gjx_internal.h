@@ -31,6 +31,40 @@ struct alignas(64) StepParams {
   unsigned split;               // CTAs per block pair (a cluster): 1 or 2
 };
 
+// one matrix of a batch: its step parameters (step unused) and D
+struct alignas(64) BatchMat {
+  StepParams p;
+  double *D;
+  unsigned steps1; // outer steps per sweep of this matrix
+};
+
+// one outer-step launch of a batch
+struct BatchStep {
+  const BatchMat *mats;
+  const uint32_t *items; // (matrix << 16) | pair of this step, largest matrices first
+  unsigned nitems, step;
+  unsigned *queue;       // work-queue heads, one per step index
+  const uint32_t *done;  // converged or failed matrices (skipped)
+  const int *err;        // any nonzero: stop
+};
+
+// end-of-sweep bookkeeping of a batch
+struct BatchSweep {
+  unsigned long long *cvg; // per matrix, (big << 32) | small of the sweep
+  uint32_t *done;
+  unsigned *sweeps;
+  unsigned long long *glb_s, *glb_b;
+  unsigned *queue;
+  unsigned *active; // matrices still sweeping after this sweep
+  unsigned nmat, nqueue;
+};
+
+cudaError_t batch_configure();
+cudaError_t launch_batch_step(bool sort, bool accv, const BatchStep &b, unsigned ctas, cudaStream_t s);
+cudaError_t launch_batch_sweep_end(const BatchSweep &w, cudaStream_t s);
+cudaError_t launch_batch_initV(const BatchMat *m, unsigned nmat, cudaStream_t s);
+cudaError_t launch_batch_initD(const BatchMat *m, unsigned nmat, const uint32_t *ok, cudaStream_t s);
+
 // TMA tensor maps for the update staging (3-D view, box {34, 8, 16}); 0 or a CUDA error
 cudaError_t make_update_map(CUtensorMap *tm, const double *base, unsigned nrow, unsigned ncol, unsigned ld);
 

@@ -460,9 +460,9 @@ __device__ __forceinline__ void update_stage(const double *const st, const doubl
 // The block-pair step kernel.
 // ---------------------------------------------------------------------------
 template <bool SORT, bool ACCV, unsigned NSPLIT>
-__global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_constant__ StepParams P)
+__device__ __forceinline__ void pair_step(const StepParams &P, const unsigned step, const unsigned pair,
+                                          const unsigned rank, double *const sm)
 {
-  extern __shared__ __align__(128) double sm[];
   double *const stg = sm;
   double *const R = sm + kOffR;
   double *const Vl = sm + kOffVl;
@@ -473,9 +473,7 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
   Rot *const rots = reinterpret_cast<Rot *>(sm + kOffRots);
 
   const unsigned tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
-  const unsigned rank = (NSPLIT > 1u) ? (blockIdx.x % NSPLIT) : 0u;
-  const unsigned pair = blockIdx.x / NSPLIT;
-  const size_t pidx = ((size_t)P.step * P.pairs + pair) * 2u;
+  const size_t pidx = ((size_t)step * P.pairs + pair) * 2u;
   const unsigned iBlk = P.strat1[pidx + 0u], jBlk = P.strat1[pidx + 1u];
   double *const Gi = P.G + (size_t)iBlk * kNColB * P.ldG;
   double *const Gj = P.G + (size_t)jBlk * kNColB * P.ldG;
@@ -719,6 +717,74 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
   }
 }
 
+// one launch per outer step: block pair blockIdx.x / NSPLIT, cluster rank
+// blockIdx.x % NSPLIT
+template <bool SORT, bool ACCV, unsigned NSPLIT>
+__global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_constant__ StepParams P)
+{
+  extern __shared__ __align__(128) double sm[];
+  const unsigned rank = (NSPLIT > 1u) ? (blockIdx.x % NSPLIT) : 0u;
+  pair_step<SORT, ACCV, NSPLIT>(P, P.step, blockIdx.x / NSPLIT, rank, sm);
+}
+
+// ---------------------------------------------------------------------------
+// Batched form: one launch per outer step index for a whole batch of
+// independent matrices.  A persistent grid (one CTA per SM) takes the step's
+// block pairs -- (matrix << 16) | pair, largest matrices first -- from a
+// work queue; each is processed by pair_step exactly as in the single-matrix
+// launch with one CTA per pair, so every matrix gets the bits it would get
+// alone.  Matrices already converged are skipped.  The mbarriers are
+// invalidated after each pair (pair_step initialises them).
+// ---------------------------------------------------------------------------
+template <bool SORT, bool ACCV>
+__global__ void __launch_bounds__(kThreads, 1) l1_batch_kernel(const __grid_constant__ BatchStep B)
+{
+  extern __shared__ __align__(128) double sm[];
+  __shared__ unsigned item;
+  uint64_t *const bars = reinterpret_cast<uint64_t *>(sm + kOffBar);
+  for (;;) {
+    if (threadIdx.x == 0u)
+      item = atomicAdd(B.queue + B.step, 1u);
+    __syncthreads();
+    const unsigned it = item;
+    const bool stop = (it >= B.nitems) || (*(volatile int *)B.err != 0);
+    __syncthreads(); // every thread has read item
+    if (stop)
+      break;
+    const uint32_t e = B.items[it];
+    const unsigned b = e >> 16u, pair = e & 0xffffu;
+    if (B.done[b])
+      continue;
+    pair_step<SORT, ACCV, 1u>(B.mats[b].p, B.step, pair, 0u, sm);
+    __syncthreads();
+    if (threadIdx.x == 0u)
+      for (unsigned k = 0u; k < 8u; ++k)
+        mbar_inval(&bars[k]);
+    __syncthreads();
+  }
+}
+
+// end of a sweep of the batch: per-matrix totals, convergence (no big
+// rotation in the sweep, or the sweep cap), the next sweep's queues cleared
+__global__ void batch_sweep_end_kernel(const BatchSweep S)
+{
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < S.nqueue)
+    S.queue[i] = 0u;
+  if (i >= S.nmat || S.done[i])
+    return;
+  const unsigned long long c = S.cvg[i];
+  S.cvg[i] = 0ull;
+  const unsigned small = (unsigned)c, big = (unsigned)(c >> 32u);
+  S.glb_s[i] += small;
+  S.glb_b[i] += big;
+  const unsigned sw = ++S.sweeps[i];
+  if (!big || sw >= kNSweep)
+    S.done[i] = 1u;
+  else
+    atomicAdd(S.active, 1u);
+}
+
 // ---------------------------------------------------------------------------
 // U = G diag(1/||g_c||), D_c = +-||g_c||^2 (share/device_code_common.hpp:187-219)
 // ---------------------------------------------------------------------------
@@ -749,6 +815,45 @@ __global__ void initV_kernel(double *const V, const unsigned ncol, const unsigne
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const unsigned c = (unsigned)(i / ncol), r = (unsigned)(i % ncol);
     V[(size_t)c * ldV + r] = (r == c) ? 1.0 : 0.0;
+  }
+}
+
+// initD for a batch: block b normalises the columns of matrix b, one warp
+// per column, the same arithmetic as initD_kernel
+__global__ void __launch_bounds__(256) initD_batch_kernel(const BatchMat *const M, const unsigned nmat,
+                                                          const uint32_t *const done_ok)
+{
+  const BatchMat &m = M[blockIdx.x];
+  if (blockIdx.x >= nmat || !done_ok[blockIdx.x])
+    return;
+  const unsigned l = threadIdx.x & 31u;
+  for (unsigned c = threadIdx.x >> 5; c < m.p.ncol; c += blockDim.x >> 5) {
+    double *const g = m.p.G + (size_t)c * m.p.ldG;
+    double x = +0.0;
+    for (unsigned r = l; r < m.p.nrow; r += 32u) {
+      const double y = g[r];
+      x = __fma_rn(y, y, x);
+    }
+    const double y = sum32(x);
+    const double nrm = __dsqrt_rn(y);
+    for (unsigned r = l; r < m.p.nrow; r += 32u)
+      g[r] = __ddiv_rn(g[r], nrm);
+    if (!l)
+      m.D[c] = (c < m.p.nplus) ? y : -y;
+  }
+}
+
+__global__ void initV_batch_kernel(const BatchMat *const M, const unsigned nmat)
+{
+  for (unsigned b = blockIdx.y; b < nmat; b += gridDim.y) {
+    const BatchMat &m = M[b];
+    if (!m.p.V)
+      continue;
+    const size_t n = (size_t)m.p.ncol * m.p.ncol;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+      const unsigned c = (unsigned)(i / m.p.ncol), r = (unsigned)(i % m.p.ncol);
+      m.p.V[(size_t)c * m.p.ldV + r] = (r == c) ? 1.0 : 0.0;
+    }
   }
 }
 
@@ -818,6 +923,57 @@ template <bool S, bool A, unsigned N> static cudaError_t launch(const StepParams
   cfg.attrs = at;
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, l1_step_kernel<S, A, N>, p);
+}
+
+template <bool S, bool A> static cudaError_t set_smem_batch(const int bytes)
+{
+  return cudaFuncSetAttribute(l1_batch_kernel<S, A>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+cudaError_t batch_configure()
+{
+  const int b = (int)l1_smem_bytes();
+  cudaError_t e;
+  if ((e = set_smem_batch<false, false>(b)) || (e = set_smem_batch<false, true>(b)) ||
+      (e = set_smem_batch<true, false>(b)) || (e = set_smem_batch<true, true>(b)))
+    return e;
+  return cudaSuccess;
+}
+
+cudaError_t launch_batch_step(const bool sort, const bool accv, const BatchStep &b, const unsigned ctas,
+                              cudaStream_t s)
+{
+  const size_t sm = l1_smem_bytes();
+  if (sort) {
+    if (accv)
+      l1_batch_kernel<true, true><<<ctas, kThreads, sm, s>>>(b);
+    else
+      l1_batch_kernel<true, false><<<ctas, kThreads, sm, s>>>(b);
+  }
+  else if (accv)
+    l1_batch_kernel<false, true><<<ctas, kThreads, sm, s>>>(b);
+  else
+    l1_batch_kernel<false, false><<<ctas, kThreads, sm, s>>>(b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_sweep_end(const BatchSweep &w, cudaStream_t s)
+{
+  const unsigned n = (w.nmat > w.nqueue) ? w.nmat : w.nqueue;
+  batch_sweep_end_kernel<<<(n + 255u) / 256u, 256u, 0, s>>>(w);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_initV(const BatchMat *m, unsigned nmat, cudaStream_t s)
+{
+  initV_batch_kernel<<<dim3(8u, nmat < 4096u ? nmat : 4096u), 256u, 0, s>>>(m, nmat);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_initD(const BatchMat *m, unsigned nmat, const uint32_t *ok, cudaStream_t s)
+{
+  initD_batch_kernel<<<nmat, 256u, 0, s>>>(m, nmat, ok);
+  return cudaGetLastError();
 }
 
 unsigned l1_split(const unsigned pairs)

@@ -76,6 +76,24 @@ int gjx_strat_info(unsigned *strat0, unsigned *steps0, unsigned *pairs0, unsigne
  * number of entries copied (<= cap), or < 0. */
 int gjx_get_strat1(unsigned short *out, unsigned cap);
 
+/*
+ * Batched form (no counterpart in the reference): nmat independent
+ * decompositions of device-resident matrices, each given exactly as
+ * gjx_hypJacL2_dev would give it alone (same bits, sweeps and counts), run
+ * together -- one launch per outer step index for the whole batch, a sweep's
+ * launches replayed from a CUDA graph, converged matrices skipped.  Per
+ * matrix b: nrow[b], ncol[b], nplus[b], dG[b] (lddG[b]), dV[b] (lddV[b];
+ * ALG & 2), dD[b]; outputs sweeps[b], glb_s[b], glb_b[b] and info[b] (0, or
+ * the argument code of gjx_hypJacL2_dev: that matrix is left untouched).
+ * The outer table of each matrix is the loaded family's (init_strats) for
+ * n1 = ncol[b] / 16, read from the same strategy library.  Returns 0, -1
+ * (bad batch arguments), GJX_ERR_NO_STRAT, GJX_ERR_CUDA or GJX_ERR_DEVICE.
+ */
+int gjx_hypJacL2_batched(unsigned routine, unsigned nmat, const unsigned *nrow, const unsigned *ncol,
+                         const unsigned *nplus, double *const *dG, const unsigned *lddG, double *const *dV,
+                         const unsigned *lddV, double *const *dD, void *stream, unsigned *sweeps,
+                         unsigned long long *glb_s, unsigned long long *glb_b, int *info);
+
 /* Make dev the calling thread's current device; returns its compute
  * capability as 10 * major + minor (100 for a B200), or -1.  Stands in for
  * configureGPU (share/cuda_helper.cu:5-54) minus its process-wide device
