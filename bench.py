@@ -56,6 +56,12 @@ WORKLOADS = {
                metric="HSVD matrices/s (2048x1024 FP64, J = diag(+I_512, -I_512), full)",
                workload="hyperbolic SVD 2048x1024, G = B diag(d), B i.i.d. N(0,1), d_j = 10^U(-6,0), seed 1002, "
                         "NPLUS=512, cycwor/cycwor, ALG 11 (U, V, D), one step = one decomposition to convergence"),
+    "c5": dict(m=0, n=0, nplus=0, alg=11, seed=5000, gen="batch", kw={}, count=4096,
+               metric="(H)SVD matrices/s, batch of 4096 FP64 matrices n x n, n uniform in {64, ..., 512}",
+               workload="batch of 4096 independent decompositions, n uniform in {64, 128, ..., 512} (PCG64 seed "
+                        "5000), G = Q1 diag(s) Q2^T, Haar Q1/Q2 (QR of Gaussians, torch CUDA generator seed 5000), "
+                        "s geometric 1..1e-6; even-indexed matrices NPLUS = n (SVD), odd NPLUS = n/2 (HSVD); "
+                        "cycwor tables of each n; ALG 11; one step = the whole batch to convergence"),
 }
 W = 32
 
@@ -64,6 +70,9 @@ def _use(name: str) -> None:
     """Bind the module-level workload constants to WORKLOADS[name]."""
     global WL, M, N, NPLUS, ALG, SEED, N1, PAIRS, STEPS1, FLOP_PER_PAIR, BYTES_PER_PAIR, METRIC, CONFIG
     WL = WORKLOADS[name]
+    if WL["gen"] == "batch":
+        WL = dict(WORKLOADS["c2"], **{k: v for k, v in WORKLOADS[name].items() if k in ("metric", "workload")})
+        WL.update(alg=WORKLOADS[name]["alg"], seed=WORKLOADS[name]["seed"])
     M, N, NPLUS, ALG, SEED = WL["m"], WL["n"], WL["nplus"], WL["alg"], WL["seed"]
     N1 = N // 16
     PAIRS = N1 // 2
@@ -227,10 +236,69 @@ def ref_gpu_once(G0: np.ndarray):
             "matrices_per_s_wall": 1.0 / t[0], "build": "reference sources, nvcc -arch sm_100a -DUSE_RSQRT -O3"}
 
 
+def reference_arm_batch(args):
+    """c5 on the reference path: per n, one decomposition by the CPU oracle
+    port (all host threads) and one by the reference's own sm_100a build,
+    each scaled by how many matrices of that n the batch holds."""
+    from oracle import oracle as O
+    from gpujachx_b200 import STRAT_PATH, synth
+    cfg = WORKLOADS["c5"]
+    sizes = batch_sizes(cfg["count"], cfg["seed"])
+    O.build()
+    cores = os.cpu_count() or 1
+    s0 = O.load_strat(STRAT_PATH, "cycwor", 32)
+    vals, ref_by, cpu_by = [], {}, {}
+    for _ in range(max(1, args.steps)):
+        tot = 0.0
+        for n in sorted(set(int(x) for x in sizes)):
+            cnt = int((sizes == n).sum())
+            G = synth.make("svd_synth", n, n, cfg["seed"] + n, smin=1e-6)
+            s1 = O.load_strat(STRAT_PATH, "cycwor", n // 16)
+            per = 0.0
+            for npl in (n, n // 2):           # half SVD, half HSVD
+                t0 = time.perf_counter()
+                r = O.hypjac_l2(ALG, G, npl, s0, s1, nthreads=cores)
+                per += 0.5 * (time.perf_counter() - t0)
+            cpu_by[n] = per
+            tot += per * cnt
+        vals.append(len(sizes) / tot)
+    try:
+        from tests.golden.make_golden import HARNESS, case, run_ref
+        if os.path.exists(HARNESS["base"]):
+            tref = 0.0
+            for n in sorted(set(int(x) for x in sizes)):
+                G = synth.make("svd_synth", n, n, cfg["seed"] + n, smin=1e-6)
+                out = run_ref(case("c5", n, n, n, ALG, seed=0), G)
+                ref_by[n] = out["timing"][0]
+                tref += out["timing"][0] * int((sizes == n).sum())
+            ref = {"matrices_per_s_wall": len(sizes) / tref, "s_per_matrix_wall_by_n": ref_by,
+                   "sample": "one SVD per n through the reference's hypJacL2 (oracle/_ref/ref_harness), scaled",
+                   "build": "reference sources, nvcc -arch sm_100a -DUSE_RSQRT -O3"}
+        else:
+            ref = None
+    except Exception as e:  # noqa: BLE001
+        ref = {"error": str(e)[:200]}
+    v = statistics.median(vals)
+    line = {"metric": cfg["metric"], "value": v, "unit": "matrices/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * len(sizes) / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "name": "c5", "count": len(sizes), "alg": ALG},
+            "cpu_baseline": {"value": v, "unit": "matrices/s", "cores": cores, "kind": "port",
+                             "sample": "one SVD and one HSVD (NPLUS = n/2) per n by the oracle port, scaled by "
+                                       "the batch's count of each n", "seconds_by_n": cpu_by},
+            "e2e": {"value": v, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if ref is not None:
+        line["ref_sm100a"] = ref
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if args.config == "c5":
+        return reference_arm_batch(args)
     _use(args.config)
     G0 = _input()
     sweeps = int(os.environ.get("GJX_BENCH_SWEEPS", "0"))
@@ -263,6 +331,182 @@ def reference_arm(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the batched workload (c5)
+# ---------------------------------------------------------------------------
+def batch_sizes(count: int = 4096, seed: int = 5000) -> np.ndarray:
+    return 64 * np.random.default_rng(seed).integers(1, 9, size=count)
+
+
+def batch_inputs(sizes, dev, seed: int = 5000):
+    """One contiguous device buffer holding every G (column major, ld = n),
+    generated on the GPU: Haar Q1, Q2 from QR of Gaussians (signs fixed by
+    diag(R)), s geometric from 1 to 1e-6, G = Q1 diag(s) Q2^T."""
+    import torch
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    offs = np.concatenate([[0], np.cumsum(sizes.astype(np.int64) ** 2)])
+    buf = torch.empty(int(offs[-1]), dtype=torch.float64, device=dev)
+    for n in sorted(set(int(x) for x in sizes)):
+        idx = np.nonzero(sizes == n)[0]
+        k = len(idx)
+
+        def haar():
+            a = torch.randn((k, n, n), dtype=torch.float64, device=dev, generator=gen)
+            q, r = torch.linalg.qr(a)
+            return q * torch.sign(torch.diagonal(r, dim1=-2, dim2=-1)).unsqueeze(-2)
+
+        q1, q2 = haar(), haar()
+        sv = torch.logspace(0.0, -6.0, n, dtype=torch.float64, device=dev)
+        g = (q1 * sv) @ q2.transpose(-2, -1)            # (k, n, n): row-major n x n = G
+        gt = g.transpose(-2, -1).contiguous()            # row j = column j of G (column major)
+        for t, b in enumerate(idx):
+            buf[int(offs[b]):int(offs[b + 1])].copy_(gt[t].reshape(-1))
+    return buf, offs
+
+
+def batch_flops_bytes(sizes, sweeps, full=True):
+    """Algorithmic FLOP and bytes of the sweeps each matrix ran (reference
+    geometry, w = 32; P_sweep = n1 (n1 - 1) / 2 cyclic block pairs)."""
+    f = b = 0.0
+    for n, sw in zip(sizes, sweeps):
+        n1 = int(n) // 16
+        p = n1 * (n1 - 1) // 2 * sw
+        f += p * (4 * n * W * W + (2 * n * W * W if full else 0))
+        b += p * (768 * n + (512 * n if full else 0))
+    return f, b
+
+
+def main_batch(args):
+    import torch
+    import torch.distributed as dist
+    import gpujachx_b200 as g
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    cfg = WORKLOADS["c5"]
+    sizes = batch_sizes(cfg["count"], cfg["seed"])
+    # weak scaling: every rank solves its own batch of the same shapes
+    G0, offs = batch_inputs(sizes, dev, cfg["seed"] + rank)
+    nplus = [int(n) if b % 2 == 0 else int(n) // 2 for b, n in enumerate(sizes)]
+    g.init_strats(None, "cycwor", 32, "cycwor", 4)
+    dG = torch.empty_like(G0)
+    dV = torch.empty_like(G0)
+    dD = torch.empty(int(sizes.sum()), dtype=torch.float64, device=dev)
+    doffs = np.concatenate([[0], np.cumsum(sizes)])
+    Gs = [dG[int(offs[b]):int(offs[b + 1])].view(int(n), int(n)) for b, n in enumerate(sizes)]
+    Vs = [dV[int(offs[b]):int(offs[b + 1])].view(int(n), int(n)) for b, n in enumerate(sizes)]
+    Ds = [dD[int(doffs[b]):int(doffs[b + 1])] for b in range(len(sizes))]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        dG.copy_(G0)
+        return g.hypJacL2_batched(ALG, Gs, nplus, Vs=Vs, Ds=Ds, stream=stream)
+
+    for _ in range(args.warmup):
+        res = step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    g.profile(False)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    prof = g.profile_read()
+    clk = clocks.stop()
+    nmat = len(sizes)
+    value, total_ms = replica_throughput(sum(times), args.steps * nmat, world, dev)
+    assert all(i == 0 for i in res.info)
+    flops, nbytes = batch_flops_bytes(sizes, res.sweeps)
+    t_s = statistics.median(times) / 1000.0
+    hbm, peak_kind = _peaks()
+    roof = {"bound": "hbm", "achieved": nbytes / t_s / 1e9, "peak": hbm, "unit": "GB/s",
+            "frac": nbytes / t_s / 1e9 / hbm, "traffic": None, "kernel": "gjx::l1_batch_kernel<true,true>",
+            "peak_kind": f"{peak_kind} HBM copy bandwidth",
+            "note": "algorithmic bytes of all sweeps run, over the device time of the whole batched call",
+            "fp64_tflops": flops / t_s / 1e12, "launches_per_step": prof["launches"] // max(1, args.steps)}
+
+    # e2e: pinned host inputs, H2D + the batched call + D2H of U, V and D, per step
+    hin = torch.empty(G0.numel(), dtype=torch.float64, pin_memory=True)
+    hin.copy_(G0)
+    hU = torch.empty_like(hin, pin_memory=True)
+    hV = torch.empty_like(hin, pin_memory=True)
+    hD = torch.empty(dD.numel(), dtype=torch.float64, pin_memory=True)
+    e2e_t = []
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dG.copy_(hin, non_blocking=True)
+        g.hypJacL2_batched(ALG, Gs, nplus, Vs=Vs, Ds=Ds, stream=stream)
+        hU.copy_(dG, non_blocking=True)
+        hV.copy_(dV, non_blocking=True)
+        hD.copy_(dD, non_blocking=True)
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            e2e_t.append(time.perf_counter() - t0)
+    e2e_v, _ = replica_throughput(sum(e2e_t) * 1000.0, args.steps * nmat, world, dev)
+    e2e = {"value": e2e_v, "unit": "matrices/s", "h2d_bytes_per_step": G0.numel() * 8,
+           "d2h_bytes_per_step": 2 * G0.numel() * 8 + dD.numel() * 8, "api": "gjx_hypJacL2_batched"}
+
+    line = {"metric": cfg["metric"], "value": value, "unit": "matrices/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "name": "c5", "count": nmat, "alg": ALG,
+                       "parallelism": ("independent batches per rank" if world > 1 else "single GPU"),
+                       "l2": "flushed between steps (256 MiB write, outside the timed events); inputs 3.4 GB > L2"},
+            "sweeps_max": max(res.sweeps), "sweeps_mean": float(np.mean(res.sweeps)), "e2e": e2e, "roofline": roof,
+            "clocks": clk, "gpu_launches": prof["launches"] // max(1, args.steps), "step_ms": times}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["plain_loop"] = plain_loop_sample(Gs, Vs, Ds, G0, offs, sizes, nplus)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def plain_loop_sample(Gs, Vs, Ds, G0, offs, sizes, nplus, per_size: int = 8):
+    """The single-matrix device call looped over a stratified sample of the
+    batch (per_size matrices of each n), scaled to the whole batch."""
+    import torch
+    import gpujachx_b200 as g
+    tot = 0.0
+    by = {}
+    for n in sorted(set(int(x) for x in sizes)):
+        idx = np.nonzero(sizes == n)[0][:per_size]
+        g.init_strats(None, "cycwor", 32, "cycwor", n // 16)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for b in idx:
+            Gs[b].view(-1).copy_(G0[int(offs[b]):int(offs[b + 1])])
+            g.hypJacL2_dev(ALG, Gs[b], nplus[b], Vs[b], Ds[b])
+        torch.cuda.synchronize()
+        per = (time.perf_counter() - t0) / len(idx)
+        by[n] = per
+        tot += per * int((sizes == n).sum())
+    g.init_strats(None, "cycwor", 32, "cycwor", 4)
+    return {"value": len(sizes) / tot, "unit": "matrices/s", "seconds_per_matrix_by_n": by,
+            "sample": f"{per_size} matrices of each n through gjx_hypJacL2_dev, scaled to the batch"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -276,6 +520,8 @@ def main():
     _use(args.config)
     if args.impl == "reference":
         return reference_arm(args)
+    if args.config == "c5":
+        return main_batch(args)
 
     import torch
     import torch.distributed as dist
