@@ -78,7 +78,7 @@ constexpr uint32_t kUpdBoxBytes = 34u * 8u * 16u * 8u;
 constexpr unsigned kRegion =
     (kGramStages * kGramStage > kUpdStages * kUpdStage) ? kGramStages * kGramStage : kUpdStages * kUpdStage;
 
-// one inner rotation, as phase B of an inner step leaves it for phase C
+// one inner rotation, as the lanes that compute it hand it to those that apply it
 struct Rot {
   double c, t, t_;
   int mode; // 0 nothing, 1 rotate, 2 swap columns
@@ -91,9 +91,7 @@ constexpr unsigned kOffVl = kOffR + 32u * kVTLd;
 constexpr unsigned kOffS0 = kOffVl + 1024u; // strat0 copy, 1024 bytes
 constexpr unsigned kOffRed = kOffS0 + 128u; // 32 unsigned
 constexpr unsigned kOffBar = kOffRed + 16u; // 8 mbarriers
-constexpr unsigned kOffProd = kOffBar + 8u;          // 16 pairs x 3 products x 33
-constexpr unsigned kOffRots = kOffProd + 16u * 3u * 33u; // 16 Rot
-constexpr unsigned kSmemDoubles = kOffRots + 16u * (sizeof(Rot) / 8u);
+constexpr unsigned kSmemDoubles = kOffBar + 8u;
 
 size_t l1_smem_bytes() { return (size_t)kSmemDoubles * sizeof(double); }
 
@@ -228,44 +226,32 @@ __device__ __forceinline__ void chol32_cta(double *const R, const unsigned tid)
 }
 
 // ---------------------------------------------------------------------------
-// Inner Jacobi sweep(s) on R (32x32) accumulating V_loc, three phases per
-// inner step (16 disjoint column pairs):
-//   A. dot products: warp w, pairs w and w + 8, lane x = row x; Dp, Dq, Apq
-//      by the reference's butterfly (sum32) -> smem;
-//   B. rotations: warp 0, lane y = pair y: relative test, trigonometric or
-//      hyperbolic rotation, sorting decision -> smem (one warp instead of
-//      sixteen computing the same scalars);
-//   C. application: warp w, pairs w and w + 8, lane x = row x.
+// Inner Jacobi sweep(s) on R (32x32) accumulating V_loc.  Per inner step (16
+// disjoint column pairs) warp w owns pairs w and w + 8, lane x = row x:
+//   the six dot products (Dp, Dq, Apq of both pairs) by register butterflies
+//   in the reference's order (share/device_code_common_Kepler.hpp:26-74:
+//   lane i adds lane i^16, ^8, ^4, ^2, ^1; IEEE addition commutes, so every
+//   lane ends with lane 0's bits); lanes 0-15 compute pair w's rotation,
+//   lanes 16-31 pair w+8's; the halves trade them with one shuffle; each lane
+//   applies both to its row of R and V_loc.  One barrier per step.
 // Every operation is the reference's (share/device_code_nosort.hpp:4-222,
 // share/device_code_cdsort.hpp:25-167, share/device_code_cdsort_KISS.hpp).
 // ---------------------------------------------------------------------------
-// Phase A: lane x stores its three products of pair y (row stride 33 keeps
-// the 16 lanes of phase B on distinct banks).
-constexpr unsigned kProdLd = 33u;
-__device__ __forceinline__ void inner_products(const double *const R, const unsigned p, const unsigned q,
-                                               const unsigned x, double *const prod)
+// rotT (trig) or rotH; when the two halves of the warp need different kinds,
+// both are computed and selected, so the warp does not run them one after
+// the other (each is a long dependent chain of divisions and square roots)
+__device__ __forceinline__ int rot_either(const bool trig, const double Apq, const double Dp, const double Dq,
+                                          double &c, double &t)
 {
-  const double Gp = E32(R, x, p), Gq = E32(R, x, q);
-  prod[0u * kProdLd + x] = __fma_rn(Gp, Gp, 0.0);
-  prod[1u * kProdLd + x] = __fma_rn(Gq, Gq, 0.0);
-  prod[2u * kProdLd + x] = __fma_rn(Gp, Gq, 0.0);
-}
-
-// The 32-lane butterfly of share/device_code_common_Kepler.hpp:26-74 (lane
-// i adds lane i^16, ^8, ^4, ^2, ^1; lane 0's result) evaluated by one thread:
-// the same additions in the same order.
-__device__ __forceinline__ double tree32(const double *const v)
-{
-  double t[16];
-#pragma unroll
-  for (unsigned i = 0u; i < 16u; ++i)
-    t[i] = v[i] + v[i + 16u];
-#pragma unroll
-  for (unsigned k = 8u; k; k >>= 1u)
-#pragma unroll
-    for (unsigned i = 0u; i < k; ++i)
-      t[i] = t[i] + t[i + k];
-  return t[0];
+  if (__all_sync(0xffffffffu, trig))
+    return rotT(Apq, Dp, Dq, c, t);
+  if (__all_sync(0xffffffffu, !trig))
+    return rotH(Apq, Dp, Dq, c, t);
+  double c1, t1, c2, t2;
+  const int b1 = rotT(Apq, Dp, Dq, c1, t1), b2 = rotH(Apq, Dp, Dq, c2, t2);
+  c = trig ? c1 : c2;
+  t = trig ? t1 : t2;
+  return trig ? b1 : b2;
 }
 
 template <bool SORT>
@@ -288,7 +274,7 @@ __device__ __forceinline__ Rot inner_rot(const double Dp, const double Dq, const
     // effects), so that its latency overlaps the relative test
     const bool trig = definite || ((p < npos) && (q < npos)) || ((p >= npos) && (q >= npos));
     double c, t;
-    const int b = trig ? rotT(Apq, Dp, Dq, c, t) : rotH(Apq, Dp, Dq, c, t);
+    const int b = rot_either(trig, Apq, Dp, Dq, c, t);
     if (ts) {
       r.c = c;
       r.t = t;
@@ -309,7 +295,7 @@ __device__ __forceinline__ Rot inner_rot(const double Dp, const double Dq, const
     else
       def = 0;
     double c, t;
-    const int b = def ? rotT(Apq, Dp, Dq, c, t) : rotH(Apq, Dp, Dq, c, t);
+    const int b = rot_either(def != 0, Apq, Dp, Dq, c, t);
     if (ts) {
       double Dp2 = Dp, Dq2 = Dq;
       r.c = c;
@@ -366,48 +352,62 @@ __device__ __forceinline__ void inner_apply(double *const R, double *const Vl, c
 template <bool SORT>
 __device__ __forceinline__ void inner_sweeps(double *const R, double *const Vl, const uint8_t *const s0,
                                              const unsigned s0steps, const unsigned nswp, const int definite,
-                                             const unsigned npos, double *const prod, Rot *const rots,
-                                             unsigned *const red, const unsigned x, const unsigned w,
-                                             unsigned &blk_s, unsigned &blk_b)
+                                             const unsigned npos, unsigned *const red, const unsigned x,
+                                             const unsigned w, unsigned &blk_s, unsigned &blk_b)
 {
   blk_s = 0u;
   blk_b = 0u;
+  const bool hb = x >= 16u; // this half computes pair w + 8 (else pair w)
   for (unsigned swp = 0u; swp < nswp; ++swp) {
-    unsigned ws = 0u, wb = 0u; // lane y of warp 0: pair y's counts
+    unsigned ws = 0u, wb = 0u; // lanes 0 and 16: their pair's counts
     for (unsigned step = 0u; step < s0steps; ++step) {
       const uint8_t *const st = s0 + step * 32u;
       const unsigned pa = st[2u * w], qa = st[2u * w + 1u], pb = st[2u * w + 16u], qb = st[2u * w + 17u];
-      inner_products(R, pa, qa, x, prod + 3u * kProdLd * w);
-      inner_products(R, pb, qb, x, prod + 3u * kProdLd * (w + 8u));
-      __syncthreads();
-      if (w == 0u) { // lanes 0-15 sum Dp of pair x, lanes 16-31 Dq of pair x-16; then Apq
-        const unsigned y = x & 15u;
-        const double *const pr = prod + 3u * kProdLd * y;
-        const double Dpq = tree32(pr + (x >> 4) * kProdLd);
-        const double Apq = tree32(pr + 2u * kProdLd);
-        const double Dq = __shfl_down_sync(0xffffffffu, Dpq, 16);
-        if (x < 16u) {
-          unsigned a, b;
-          rots[x] = inner_rot<SORT>(Dpq, Dq, Apq, st[2u * x], st[2u * x + 1u], definite, npos, a, b);
-          ws += a;
-          wb += b;
-        }
+      const double Gpa = E32(R, x, pa), Gqa = E32(R, x, qa), Gpb = E32(R, x, pb), Gqb = E32(R, x, qb);
+      double v[6] = {__fma_rn(Gpa, Gpa, 0.0), __fma_rn(Gqa, Gqa, 0.0), __fma_rn(Gpa, Gqa, 0.0),
+                     __fma_rn(Gpb, Gpb, 0.0), __fma_rn(Gqb, Gqb, 0.0), __fma_rn(Gpb, Gqb, 0.0)};
+#pragma unroll
+      for (unsigned k = 16u; k; k >>= 1u) {
+        double o[6];
+#pragma unroll
+        for (unsigned i = 0u; i < 6u; ++i)
+          o[i] = __shfl_xor_sync(0xffffffffu, v[i], k);
+#pragma unroll
+        for (unsigned i = 0u; i < 6u; ++i)
+          v[i] = v[i] + o[i];
       }
-      __syncthreads();
-      inner_apply(R, Vl, pa, qa, rots[w], x);
-      inner_apply(R, Vl, pb, qb, rots[w + 8u], x);
+      unsigned a_s, a_b;
+      const Rot r = inner_rot<SORT>(hb ? v[3] : v[0], hb ? v[4] : v[1], hb ? v[5] : v[2], hb ? pb : pa,
+                                    hb ? qb : qa, definite, npos, a_s, a_b);
+      if (x == 0u || x == 16u) {
+        ws += a_s;
+        wb += a_b;
+      }
+      Rot o;
+      o.c = __shfl_xor_sync(0xffffffffu, r.c, 16);
+      o.t = __shfl_xor_sync(0xffffffffu, r.t, 16);
+      o.t_ = __shfl_xor_sync(0xffffffffu, r.t_, 16);
+      const int fl = __shfl_xor_sync(0xffffffffu, r.mode | (r.scale << 2) | (r.swap << 3), 16);
+      o.mode = fl & 3;
+      o.scale = (fl >> 2) & 1;
+      o.swap = (fl >> 3) & 1;
+      inner_apply(R, Vl, pa, qa, hb ? o : r, x);
+      inner_apply(R, Vl, pb, qb, hb ? r : o, x);
       __syncthreads();
     }
-    if (w == 0u) {
-      ws = __reduce_add_sync(0xffffffffu, ws);
-      wb = __reduce_add_sync(0xffffffffu, wb);
-      if (x == 0u) {
-        red[0] = ws;
-        red[1] = wb;
-      }
+    ws = __reduce_add_sync(0xffffffffu, ws);
+    wb = __reduce_add_sync(0xffffffffu, wb);
+    if (x == 0u) {
+      red[2u * w] = ws;
+      red[2u * w + 1u] = wb;
     }
     __syncthreads();
-    const unsigned tot_s = red[0], tot_b = red[1];
+    unsigned tot_s = 0u, tot_b = 0u;
+#pragma unroll
+    for (unsigned k = 0u; k < kThreads / 32u; ++k) {
+      tot_s += red[2u * k];
+      tot_b += red[2u * k + 1u];
+    }
     __syncthreads();
     if (tot_s) {
       blk_s += tot_s;
@@ -469,8 +469,6 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
   uint8_t *const s0 = reinterpret_cast<uint8_t *>(sm + kOffS0);
   unsigned *const red = reinterpret_cast<unsigned *>(sm + kOffRed);
   uint64_t *const bars = reinterpret_cast<uint64_t *>(sm + kOffBar);
-  double *const prod = sm + kOffProd;
-  Rot *const rots = reinterpret_cast<Rot *>(sm + kOffRots);
 
   const unsigned tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
   const size_t pidx = ((size_t)step * P.pairs + pair) * 2u;
@@ -627,7 +625,7 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
     }
   }
   unsigned blk_s, blk_b;
-  inner_sweeps<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, prod, rots, red, lane, warp, blk_s, blk_b);
+  inner_sweeps<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, lane, warp, blk_s, blk_b);
 
   if (rank == 0u && tid == 0u && blk_s) {
     if (blk_b)
