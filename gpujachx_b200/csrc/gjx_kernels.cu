@@ -182,33 +182,46 @@ __device__ __forceinline__ bool gram_lane_of(const unsigned rank, const unsigned
 }
 
 // ---------------------------------------------------------------------------
-// Right-looking Cholesky of the lower triangle held in R, by the whole CTA
-// (compact code: it runs once per block pair, from a cold instruction
-// cache).  Column k: warp 0 divides (x > k: times rsqrt_rn(Akk)) and roots
-// the pivot; then the later columns j are updated, spread over the warps,
-// A(x,j) = fma(-A(x,k), A(j,k), A(x,j)) for x >= j.  Afterwards R = L^T
-// with zeros below the diagonal.
+// Right-looking Cholesky of the lower triangle held in R, by the whole CTA,
+// with a one-column look-ahead: in round k warp 0 updates column k+1 by
+// column k and pivots it (x > k+1: times rsqrt_rn(A(k+1,k+1)), the diagonal
+// its square root) while warps 1..7 update columns k+2..31 by column k,
+// A(x,j) = fma(-A(x,k), A(j,k), A(x,j)) for x >= j.  Every entry receives
+// the reference's operations in the reference's order
+// (share/device_code_common_Cholesky.hpp:58-158); one barrier per column.
+// Afterwards R = L^T with zeros below the diagonal.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void chol_pivot(double *const R, const unsigned j, const unsigned x, const double a)
+{
+  const double ajj = __shfl_sync(0xffffffffu, a, j);
+  const double rs = rsqrt_rn(ajj), sq = __dsqrt_rn(ajj);
+  if (x > j)
+    E32(R, x, j) = a * rs;
+  else if (x == j)
+    E32(R, j, j) = sq;
+}
+
 __device__ __forceinline__ void chol32_cta(double *const R, const unsigned tid)
 {
   const unsigned w = tid >> 5, x = tid & 31u;
+  if (w == 0u)
+    chol_pivot(R, 0u, x, E32(R, x, 0u));
+  __syncthreads();
 #pragma unroll 1
-  for (unsigned k = 0u; k < 32u; ++k) {
+  for (unsigned k = 0u; k + 1u < 32u; ++k) {
     if (w == 0u) {
-      const double akk = E32(R, k, k);
-      const double rs = rsqrt_rn(akk);
-      const double sq = __dsqrt_rn(akk);
-      __syncwarp();
-      if (x > k)
-        E32(R, x, k) = E32(R, x, k) * rs;
-      else if (x == k)
-        E32(R, k, k) = sq;
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (unsigned j = k + 1u + w; j < 32u; j += kThreads / 32u)
+      const unsigned j = k + 1u;
+      double a = E32(R, x, j);
       if (x >= j)
-        E32(R, x, j) = __fma_rn(-E32(R, x, k), E32(R, j, k), E32(R, x, j));
+        a = __fma_rn(-E32(R, x, k), E32(R, j, k), a);
+      chol_pivot(R, j, x, a);
+    }
+    else {
+#pragma unroll 1
+      for (unsigned j = k + 1u + w; j < 32u; j += kThreads / 32u - 1u)
+        if (x >= j)
+          E32(R, x, j) = __fma_rn(-E32(R, x, k), E32(R, j, k), E32(R, x, j));
+    }
     __syncthreads();
   }
   double v[4];
