@@ -56,6 +56,11 @@ WORKLOADS = {
                metric="HSVD matrices/s (2048x1024 FP64, J = diag(+I_512, -I_512), full)",
                workload="hyperbolic SVD 2048x1024, G = B diag(d), B i.i.d. N(0,1), d_j = 10^U(-6,0), seed 1002, "
                         "NPLUS=512, cycwor/cycwor, ALG 11 (U, V, D), one step = one decomposition to convergence"),
+    "c4": dict(m=8192, n=8192, nplus=8192, alg=11, seed=1003, gen="haar_gpu", kw=dict(smin=1e-12),
+               metric="SVD matrices/s (8192x8192 FP64, full SVD)",
+               workload="plain FP64 SVD 8192x8192, G = Q1 diag(s) Q2^T, Haar Q1/Q2 (QR of Gaussians, torch CUDA "
+                        "generator seed 1003), s geometric 1..1e-12, NPLUS=N, cycwor/cycwor, ALG 11 (U, V, D), "
+                        "one step = one decomposition to convergence"),
     "c5": dict(m=0, n=0, nplus=0, alg=11, seed=5000, gen="batch", kw={}, count=4096,
                metric="(H)SVD matrices/s, batch of 4096 FP64 matrices n x n, n uniform in {64, ..., 512}",
                workload="batch of 4096 independent decompositions, n uniform in {64, 128, ..., 512} (PCG64 seed "
@@ -88,6 +93,19 @@ def _use(name: str) -> None:
 
 def _input() -> np.ndarray:
     from gpujachx_b200 import synth
+    if WL["gen"] == "haar_gpu":          # too large for a CPU QR at bench start-up
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(SEED)
+
+        def haar(n):
+            q, r = torch.linalg.qr(torch.randn((n, n), dtype=torch.float64, device=dev, generator=gen))
+            return q * torch.sign(torch.diagonal(r)).unsqueeze(0)
+
+        sv = torch.logspace(0.0, float(np.log10(WL["kw"]["smin"])), N, dtype=torch.float64, device=dev)
+        G = (haar(M)[:, :N] * sv) @ haar(N).T
+        return np.asfortranarray(G.cpu().numpy())
     return synth.make(WL["gen"], M, N, SEED, **WL["kw"])
 
 
@@ -209,7 +227,10 @@ def accuracy_figures(G0: np.ndarray, U: np.ndarray, V, D: np.ndarray) -> dict:
     relative error of D against an FP64 reference spectrum -- LAPACK DGESVJ's
     sigma^2 for an SVD, eigenvalues of R J R^T (G = QR) for an HSVD."""
     from gpujachx_b200 import accuracy
-    if NPLUS == N:
+    if WL["gen"] == "haar_gpu":
+        lam = np.logspace(0.0, 2.0 * np.log10(WL["kw"]["smin"]), N)
+        ref = "the constructed spectrum s^2 (G = Q1 diag(s) Q2^T formed in FP64: absolute accuracy only)"
+    elif NPLUS == N:
         from oracle import lapack
         lam = lapack.dgesvj(G0, jobv="N", threads=os.cpu_count() or 1)[0] ** 2
         ref = "LAPACK DGESVJ sigma^2"
@@ -218,6 +239,21 @@ def accuracy_figures(G0: np.ndarray, U: np.ndarray, V, D: np.ndarray) -> dict:
         J = np.r_[np.ones(NPLUS), -np.ones(N - NPLUS)]
         lam = np.linalg.eigvalsh((R * J) @ R.T)
         ref = "eigenvalues of R J R^T, G = QR (absolute accuracy only)"
+    if M * N * N > 2 ** 34:  # too large for extended precision on the host: FP64 products on the GPU
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        Ut = torch.tensor(U, device=dev)
+        e = (Ut.T @ Ut - torch.eye(N, dtype=torch.float64, device=dev)).abs()
+        out = {"|| U^T U - I ||_M (FP64 on the GPU)": float(e.max())}
+        if V is not None:
+            Vt = torch.tensor(V, device=dev)
+            J = torch.ones(N, dtype=torch.float64, device=dev)
+            J[NPLUS:] = -1.0
+            e = ((Vt.T * J) @ Vt - torch.diag(J)).abs()
+            out["|| V^T J V - J ||_M (FP64 on the GPU)"] = float(e.max())
+        ab, rel = accuracy.derr(D, lam)
+        out.update(max_rel_err_D=float(rel[-1]), max_abs_err_D=float(ab[-1]), reference_spectrum=ref)
+        return out
     r = accuracy.pp80(U, D, V=V, nplus=NPLUS, lam=lam, uut=(M * M * N <= 2 ** 33))
     out = {lab: v for lab, v in zip(r["labels"], r["nrms"]) if v == v}
     out.update(max_rel_err_D=r["max_rel_err"], max_abs_err_D=r["max_abs_err"], reference_spectrum=ref)
@@ -391,8 +427,18 @@ def main_batch(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
     cfg = WORKLOADS["c5"]
     sizes = batch_sizes(cfg["count"], cfg["seed"])
-    # weak scaling: every rank solves its own batch of the same shapes
-    G0, offs = batch_inputs(sizes, dev, cfg["seed"] + rank)
+    if args.shard and world > 1:
+        # strong scaling: one batch, split by the size-balanced partition
+        from gpujachx_b200 import batch as B
+        G_all, offs_all = batch_inputs(sizes, dev, cfg["seed"])
+        mine = B.partition(sizes, sizes, world)[rank]
+        sizes = sizes[mine]
+        offs = np.concatenate([[0], np.cumsum(sizes.astype(np.int64) ** 2)])
+        G0 = torch.cat([G_all[int(offs_all[b]):int(offs_all[b + 1])] for b in mine])
+        del G_all
+    else:
+        # weak scaling: every rank solves its own batch of the same shapes
+        G0, offs = batch_inputs(sizes, dev, cfg["seed"] + rank)
     nplus = [int(n) if b % 2 == 0 else int(n) // 2 for b, n in enumerate(sizes)]
     g.init_strats(None, "cycwor", 32, "cycwor", 4)
     dG = torch.empty_like(G0)
@@ -434,6 +480,8 @@ def main_batch(args):
     clk = clocks.stop()
     nmat = len(sizes)
     value, total_ms = replica_throughput(sum(times), args.steps * nmat, world, dev)
+    if args.shard and world > 1:  # every rank's shard counts once: the whole batch per step
+        value = args.steps * cfg["count"] / (total_ms / 1000.0)
     assert all(i == 0 for i in res.info)
     flops, nbytes = batch_flops_bytes(sizes, res.sweeps)
     t_s = statistics.median(times) / 1000.0
@@ -468,9 +516,11 @@ def main_batch(args):
 
     line = {"metric": cfg["metric"], "value": value, "unit": "matrices/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "strong" if (args.shard and world > 1) else "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
             "config": {"workload": cfg["workload"], "name": "c5", "count": nmat, "alg": ALG,
-                       "parallelism": ("independent batches per rank" if world > 1 else "single GPU"),
+                       "parallelism": ("one batch partitioned over ranks (size-balanced)" if (args.shard and world > 1)
+                                       else "independent batches per rank" if world > 1 else "single GPU"),
                        "l2": "flushed between steps (256 MiB write, outside the timed events); inputs 3.4 GB > L2"},
             "sweeps_max": max(res.sweeps), "sweeps_mean": float(np.mean(res.sweeps)), "e2e": e2e, "roofline": roof,
             "clocks": clk, "gpu_launches": prof["launches"] // max(1, args.steps), "step_ms": times}
@@ -516,6 +566,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baselines")
     ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS), help="workload (default: the headline c2)")
     ap.add_argument("--accuracy", action="store_true", help="add pp80 figures of the last decomposition")
+    ap.add_argument("--shard", action="store_true", help="c5 over N ranks: split one batch instead of N batches")
     args = ap.parse_args()
     _use(args.config)
     if args.impl == "reference":
@@ -632,7 +683,9 @@ def main():
                                             dD.cpu().numpy())
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_port_sample(G0, sweeps)
-        if NPLUS == N:
+        if NPLUS == N and M * N > 2 ** 25:
+            line["lapack_dgesvj"] = {"skipped": "DGESVJ on the host takes about an hour at this size"}
+        elif NPLUS == N:
             try:
                 line["lapack_dgesvj"] = lapack_baseline(G0)
             except Exception as e:  # noqa: BLE001

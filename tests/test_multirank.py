@@ -50,3 +50,45 @@ def test_single_rank_is_local():
     import bench
     v, t = bench.replica_throughput(250.0, steps=2, world=1)
     assert t == 250.0 and v == pytest.approx(8.0)
+
+
+def _shard_rank(rank, world, port, q):
+    sys.path.insert(0, ROOT)
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import bench
+    from gpujachx_b200 import batch
+    sizes = bench.batch_sizes(4096, 5000)
+    parts = batch.partition(sizes, sizes, world)
+    mine = parts[rank]
+    # every rank computes the same partition; gather the shards to check
+    counts = [torch.zeros(1, dtype=torch.int64) for _ in range(world)]
+    dist.all_gather(counts, torch.tensor([len(mine)]))
+    total = torch.zeros(1, dtype=torch.float64)
+    dist.all_reduce(total.add_(float(sum(int(x) for x in mine))))
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, [int(c) for c in counts], float(total), mine.tolist(), batch.imbalance(parts, sizes, sizes)))
+
+
+def test_batch_shards_over_two_gloo_ranks():
+    """The C5 batch split over 2 ranks by the size-balanced partition: the
+    shards are disjoint, cover the batch, and carry equal work within 0.1 %."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 31500 + (os.getpid() % 2000)
+    ps = [ctx.Process(target=_shard_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(timeout=120)
+    got = sorted(q.get(timeout=10) for _ in range(2))
+    for p in ps:
+        assert p.exitcode == 0
+    (_, c0, s0, m0, imb), (_, c1, s1, m1, _) = got
+    assert c0 == c1 and sum(c0) == 4096
+    assert s0 == s1 == float(sum(range(4096)))
+    assert not set(m0) & set(m1) and len(set(m0) | set(m1)) == 4096
+    assert imb < 1.001
