@@ -35,7 +35,7 @@ EXPORTS = ("hypJacL2", "init_strats", "gjx_init_strats", "gjx_strat_info", "gjx_
            "gjx_hypJacL2_dev", "gjx_release_cache", "gjx_set_verbose", "gjx_last_error",
            "gjx_version", "gjx_rsqrt_rn_dev", "gjx_profile", "gjx_profile_read", "gjx_hypJacL2_noalloc",
            "gjx_validate_pairs", "gjx_validate_strats", "gjx_configure_device", "gjx_h5_read", "gjx_h5_write",
-           "gjx_hypJacL2_batched")
+           "gjx_hypJacL2_batched", "gjx_set_sweep_mode")
 
 
 class GjxError(RuntimeError):
@@ -96,6 +96,8 @@ def lib() -> ctypes.CDLL:
     L.gjx_hypJacL2_batched.argtypes = [u, u, pu, pu, pu, pp, pu, pp, pu, pp, ctypes.c_void_p, pu, pull, pull,
                                        ctypes.POINTER(ctypes.c_int)]
     L.gjx_hypJacL2_batched.restype = i
+    L.gjx_set_sweep_mode.argtypes = [i]
+    L.gjx_set_sweep_mode.restype = None
     L.gjx_configure_device.argtypes = [i]
     L.gjx_configure_device.restype = i
     L.gjx_set_verbose(0)

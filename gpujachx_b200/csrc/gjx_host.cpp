@@ -46,6 +46,7 @@ struct Strat {
 std::mutex g_mtx;
 Strat g_strat;
 int g_verbose = 1;
+int g_sweep_mode = 1; // 1: one launch per sweep where every cluster fits; 0: one launch per outer step
 
 // profiling: launch counts always; with g_prof, CUDA events around every
 // block-pair launch, read back at the end of each sweep
@@ -94,6 +95,7 @@ struct DevCtx {
   unsigned long long version = ~0ull;
   unsigned long long *d_cnt = nullptr; // [0] = cvg, [1] = err (int in the low word)
   unsigned long long *h_cnt = nullptr; // pinned mirror
+  unsigned *d_ver = nullptr;           // per-block write counts of the one-launch sweep (1024 blocks)
   // outer tables of the batched form, by n1, for strategy version btab_version
   bool batch_ready = false;
   cudaStream_t batch_stream = nullptr; // graphs cannot be captured on the legacy default stream
@@ -130,6 +132,7 @@ int dev_ctx(DevCtx *&ctx)
     GJX_CUDA(gjx::l1_configure(), "l1_configure");
     GJX_CUDA(cudaMalloc(&ctx->d_s0, 32u * 16u * 2u), "cudaMalloc(strat0)");
     GJX_CUDA(cudaMalloc(&ctx->d_cnt, 2u * sizeof(unsigned long long)), "cudaMalloc(counters)");
+    GJX_CUDA(cudaMalloc(&ctx->d_ver, 1024u * sizeof(unsigned)), "cudaMalloc(block counts)");
     GJX_CUDA(cudaHostAlloc(&ctx->h_cnt, 2u * sizeof(unsigned long long), cudaHostAllocPortable),
              "cudaHostAlloc(counters)");
     ctx->ready = true;
@@ -172,7 +175,8 @@ double secs(const clk::time_point a, const clk::time_point b)
 int run_sweeps_core(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
                     double *const dG, const unsigned lddG, double *const dV, const unsigned lddV, double *const dD,
                     const cudaStream_t st, const uint8_t *const d_s0, const uint16_t *const d_s1,
-                    unsigned long long *const d_cnt, unsigned long long *const h_cnt, const bool prof,
+                    unsigned long long *const d_cnt, unsigned long long *const h_cnt, unsigned *const d_ver,
+                    const bool prof,
                     unsigned *const glbSwp, unsigned long long *const glb_s, unsigned long long *const glb_b)
 {
   const bool cdsort = (routine & GJX_CDSORT_1) != 0u, full = (routine & GJX_FULL_SVD) != 0u,
@@ -214,24 +218,46 @@ int run_sweeps_core(const unsigned routine, const unsigned nrow, const unsigned 
   *glb_b = 0ull;
   unsigned blk_swp = 0u;
   clk::time_point ts = clk::now();
+  p.steps1 = g_strat.steps1;
+  p.ver = d_ver;
+  // one launch per sweep when all clusters of a step are resident together
+  bool one_launch = d_ver && g_sweep_mode && g_strat.n1 <= 1024u && gjx::sweep_kernel_fits(cdsort, full, p);
   while (blk_swp < gjx::kNSweep) {
     GJX_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st), "clear counter");
-    for (unsigned stp = 0u; stp < g_strat.steps1; ++stp) {
-      p.step = stp;
+    if (one_launch) {
+      GJX_CUDA(cudaMemsetAsync(d_ver, 0, g_strat.n1 * sizeof(unsigned), st), "clear block counts");
       if (prof)
-        GJX_CUDA(cudaEventRecord(g_prof.ev[2u * stp], st), "cudaEventRecord");
-      GJX_CUDA(gjx::launch_l1_step(cdsort, full, p, st), "block-pair step");
+        GJX_CUDA(cudaEventRecord(g_prof.ev[0], st), "cudaEventRecord");
+      const cudaError_t le = gjx::launch_l1_sweep(cdsort, full, p, st);
+      if (le != cudaSuccess && blk_swp == 0u) { // refused (a cooperative launch that does not fit): per step
+        (void)cudaGetLastError();
+        one_launch = false;
+      }
+      else
+        GJX_CUDA(le, "block-pair sweep");
       if (prof)
-        GJX_CUDA(cudaEventRecord(g_prof.ev[2u * stp + 1u], st), "cudaEventRecord");
+        GJX_CUDA(cudaEventRecord(g_prof.ev[1], st), "cudaEventRecord");
+      if (one_launch)
+        g_prof.launches += 1u;
     }
-    g_prof.launches += g_strat.steps1;
+    if (!one_launch) {
+      for (unsigned stp = 0u; stp < g_strat.steps1; ++stp) {
+        p.step = stp;
+        if (prof)
+          GJX_CUDA(cudaEventRecord(g_prof.ev[2u * stp], st), "cudaEventRecord");
+        GJX_CUDA(gjx::launch_l1_step(cdsort, full, p, st), "block-pair step");
+        if (prof)
+          GJX_CUDA(cudaEventRecord(g_prof.ev[2u * stp + 1u], st), "cudaEventRecord");
+      }
+      g_prof.launches += g_strat.steps1;
+    }
     g_prof.l1_launches += g_strat.steps1;
     ++blk_swp;
     GJX_CUDA(cudaMemcpyAsync(h_cnt, d_cnt, 2u * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
              "read counters");
     GJX_CUDA(cudaStreamSynchronize(st), "sweep");
     if (prof)
-      for (unsigned stp = 0u; stp < g_strat.steps1; ++stp) {
+      for (unsigned stp = 0u; stp < (one_launch ? 1u : g_strat.steps1); ++stp) { // (steps: events 2 stp, 2 stp + 1)
         float ms = 0.0f;
         GJX_CUDA(cudaEventElapsedTime(&ms, g_prof.ev[2u * stp], g_prof.ev[2u * stp + 1u]), "cudaEventElapsedTime");
         g_prof.l1_ms += ms;
@@ -277,7 +303,7 @@ int run_sweeps(const unsigned routine, const unsigned nrow, const unsigned ncol,
   if (const int r = upload_strat(*ctx, st))
     return r;
   return run_sweeps_core(routine, nrow, ncol, nplus, dG, lddG, dV, lddV, dD, st, ctx->d_s0, ctx->d_s1, ctx->d_cnt,
-                         ctx->h_cnt, g_prof.on, glbSwp, glb_s, glb_b);
+                         ctx->h_cnt, ctx->d_ver, g_prof.on, glbSwp, glb_s, glb_b);
 }
 
 // argument checks of 1/HypJacL2.cu:39-77, same codes in the same order
@@ -629,7 +655,8 @@ int noalloc_sweeps(const unsigned routine, const unsigned nrow, const unsigned n
   return run_sweeps_core(routine, nrow, ncol, nplus, dG, lddG, dV, lddV, dD, st,
                          reinterpret_cast<const uint8_t *>(base + kScrS0),
                          reinterpret_cast<const uint16_t *>(base + kScrS1),
-                         reinterpret_cast<unsigned long long *>(base + kScrCnt), h_cnt, false, glbSwp, glb_s, glb_b);
+                         reinterpret_cast<unsigned long long *>(base + kScrCnt), h_cnt, nullptr, false, glbSwp, glb_s,
+                         glb_b);
 }
 
 int check_dev_args(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
@@ -1009,6 +1036,12 @@ int gjx_hypJacL2_batched(const unsigned routine, const unsigned nmat, const unsi
   }
   return run_batch(routine, nmat, nrow, ncol, nplus, dG, lddG, dV, lddV, dD, static_cast<cudaStream_t>(stream),
                    sweeps, glb_s, glb_b, info);
+}
+
+void gjx_set_sweep_mode(const int mode)
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  g_sweep_mode = mode ? 1 : 0;
 }
 
 } // extern "C"

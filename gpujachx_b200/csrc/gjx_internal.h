@@ -29,6 +29,8 @@ struct alignas(64) StepParams {
   unsigned nswp0;               // inner sweeps per block pair (1 or 30)
   int gdefinite;                // +1 J = I, -1 J = -I, 0 mixed signs
   unsigned split;               // CTAs per block pair (a cluster): 1 or 2
+  unsigned steps1;              // outer steps per sweep (persistent sweep kernel)
+  unsigned *ver;                // per block: CTAs that have finished writing it this sweep
 };
 
 // one matrix of a batch: its step parameters (step unused) and D
@@ -60,6 +62,10 @@ struct BatchSweep {
 };
 
 cudaError_t batch_configure();
+// one launch for a whole sweep (all outer steps), when every cluster of the
+// step fits on the GPU at once; false when it does not (launch per step)
+bool sweep_kernel_fits(bool sort, bool accv, const StepParams &p);
+cudaError_t launch_l1_sweep(bool sort, bool accv, const StepParams &p, cudaStream_t s);
 cudaError_t launch_batch_step(bool sort, bool accv, const BatchStep &b, unsigned ctas, cudaStream_t s);
 cudaError_t launch_batch_sweep_end(const BatchSweep &w, cudaStream_t s);
 cudaError_t launch_batch_initV(const BatchMat *m, unsigned nmat, cudaStream_t s);

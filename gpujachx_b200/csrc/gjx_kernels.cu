@@ -739,6 +739,75 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
 }
 
 // ---------------------------------------------------------------------------
+// One launch for a whole sweep.  Cluster c takes block pair c of every outer
+// step in turn.  A block is rewritten by exactly one pair per step, so pair
+// (i, j) of step s may start once both blocks have been written by all CTAs
+// of their step s-1 pairs: P.ver counts those CTAs (NSPLIT per step).
+// Thread 0 of each CTA waits for the counts (bounded); the CTAs of a cluster
+// agree through distributed shared memory and a cluster barrier, so they
+// leave together on an error (pair_step has one cluster barrier on every
+// path).  Writers fence their stores before counting; readers acquire the
+// counts and fence the async proxy before their tile copies.  All clusters
+// are resident at once (cooperative launch, checked on the host).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+template <bool SORT, bool ACCV, unsigned NSPLIT>
+__global__ void __launch_bounds__(kThreads, 1) l1_sweep_kernel(const __grid_constant__ StepParams P)
+{
+  extern __shared__ __align__(128) double sm[];
+  __shared__ unsigned agree[2]; // [0] this CTA may proceed, [1] the peer CTA may
+  uint64_t *const bars = reinterpret_cast<uint64_t *>(sm + kOffBar);
+  const unsigned rank = (NSPLIT > 1u) ? (blockIdx.x % NSPLIT) : 0u;
+  const unsigned pair = blockIdx.x / NSPLIT;
+  for (unsigned step = 0u; step < P.steps1; ++step) {
+    const size_t pidx = ((size_t)step * P.pairs + pair) * 2u;
+    const unsigned iB = P.strat1[pidx + 0u], jB = P.strat1[pidx + 1u];
+    if (threadIdx.x == 0u) {
+      const unsigned need = NSPLIT * step;
+      unsigned ok = (*(volatile int *)P.err == 0) ? 1u : 0u;
+      const long long t0 = clock64();
+      while (ok && (ld_acquire(P.ver + iB) < need || ld_acquire(P.ver + jB) < need)) {
+        if (*(volatile int *)P.err)
+          ok = 0u;
+        else if (clock64() - t0 > kWaitLimit) {
+          atomicOr(P.err, kErrWaitTimeout);
+          ok = 0u;
+        }
+        else
+          __nanosleep(64);
+      }
+      agree[0] = ok;
+      if (NSPLIT > 1u)
+        cg::this_cluster().map_shared_rank(agree, rank ^ 1u)[1] = ok;
+    }
+    if (NSPLIT > 1u)
+      cg::this_cluster().sync();
+    else
+      __syncthreads();
+    if (!agree[0] || (NSPLIT > 1u && !agree[1]))
+      break; // the same decision in every CTA of the cluster
+    asm volatile("fence.proxy.async;" ::: "memory"); // the copies below read what other SMs wrote
+    pair_step<SORT, ACCV, NSPLIT>(P, step, pair, rank, sm);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0u) {
+      __threadfence();
+      atomicAdd(P.ver + iB, 1u);
+      atomicAdd(P.ver + jB, 1u);
+      for (unsigned k = 0u; k < 8u; ++k)
+        mbar_inval(&bars[k]);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Batched form: one launch per outer step index for a whole batch of
 // independent matrices.  A persistent grid (one CTA per SM) takes the step's
 // block pairs -- (matrix << 16) | pair, largest matrices first -- from a
@@ -985,6 +1054,72 @@ cudaError_t launch_batch_initD(const BatchMat *m, unsigned nmat, const uint32_t 
 {
   initD_batch_kernel<<<nmat, 256u, 0, s>>>(m, nmat, ok);
   return cudaGetLastError();
+}
+
+template <bool S, bool A, unsigned N> static cudaLaunchConfig_t sweep_cfg(const StepParams &p, cudaStream_t s,
+                                                                         cudaLaunchAttribute *at)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(p.pairs * N);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = l1_smem_bytes();
+  cfg.stream = s;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = N;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeCooperative;
+  at[1].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 2;
+  return cfg;
+}
+
+template <bool S, bool A, unsigned N> static bool sweep_fits(const StepParams &p)
+{
+  if (cudaFuncSetAttribute(l1_sweep_kernel<S, A, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)l1_smem_bytes()) != cudaSuccess)
+    return false;
+  cudaLaunchAttribute at[2];
+  cudaLaunchConfig_t cfg = sweep_cfg<S, A, N>(p, nullptr, at);
+  cfg.numAttrs = 1; // the occupancy query takes the cluster shape
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, l1_sweep_kernel<S, A, N>, &cfg) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return (unsigned)clusters >= p.pairs;
+}
+
+template <bool S, bool A, unsigned N> static cudaError_t sweep_launch(const StepParams &p, cudaStream_t s)
+{
+  cudaLaunchAttribute at[2];
+  cudaLaunchConfig_t cfg = sweep_cfg<S, A, N>(p, s, at);
+  return cudaLaunchKernelEx(&cfg, l1_sweep_kernel<S, A, N>, p);
+}
+
+bool sweep_kernel_fits(const bool sort, const bool accv, const StepParams &p)
+{
+  if (p.split == 2u) {
+    if (sort)
+      return accv ? sweep_fits<true, true, 2u>(p) : sweep_fits<true, false, 2u>(p);
+    return accv ? sweep_fits<false, true, 2u>(p) : sweep_fits<false, false, 2u>(p);
+  }
+  if (sort)
+    return accv ? sweep_fits<true, true, 1u>(p) : sweep_fits<true, false, 1u>(p);
+  return accv ? sweep_fits<false, true, 1u>(p) : sweep_fits<false, false, 1u>(p);
+}
+
+cudaError_t launch_l1_sweep(const bool sort, const bool accv, const StepParams &p, cudaStream_t s)
+{
+  if (p.split == 2u) {
+    if (sort)
+      return accv ? sweep_launch<true, true, 2u>(p, s) : sweep_launch<true, false, 2u>(p, s);
+    return accv ? sweep_launch<false, true, 2u>(p, s) : sweep_launch<false, false, 2u>(p, s);
+  }
+  if (sort)
+    return accv ? sweep_launch<true, true, 1u>(p, s) : sweep_launch<true, false, 1u>(p, s);
+  return accv ? sweep_launch<false, true, 1u>(p, s) : sweep_launch<false, false, 1u>(p, s);
 }
 
 unsigned l1_split(const unsigned pairs)

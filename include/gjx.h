@@ -94,6 +94,13 @@ int gjx_hypJacL2_batched(unsigned routine, unsigned nmat, const unsigned *nrow, 
                          const unsigned *lddV, double *const *dD, void *stream, unsigned *sweeps,
                          unsigned long long *glb_s, unsigned long long *glb_b, int *info);
 
+/* How a sweep is launched: 1 (default) one launch per sweep, in which the
+ * block pairs of consecutive outer steps start as soon as their two blocks
+ * are written (used when all clusters of a step fit on the GPU at once,
+ * else per step); 0 one launch per outer step, as the reference.  The
+ * results are the same bits either way. */
+void gjx_set_sweep_mode(int mode);
+
 /* Make dev the calling thread's current device; returns its compute
  * capability as 10 * major + minor (100 for a B200), or -1.  Stands in for
  * configureGPU (share/cuda_helper.cu:5-54) minus its process-wide device
