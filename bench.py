@@ -632,16 +632,20 @@ def main():
     clk = clocks.stop()
     value, total_ms = replica_throughput(sum(times), args.steps, world, dev)
 
-    # roofline of the block-pair kernel
+    # roofline of the block-pair kernel (one launch per sweep when it fits: fewer launches than steps)
+    one_launch = prof["launches"] < prof["l1_launches"]
     l1_mean_s = prof["l1_ms"] / max(1, prof["l1_launches"]) / 1000.0
     hbm, peak_kind = _peaks()
     ach = BYTES_PER_PAIR * PAIRS / l1_mean_s / 1e9
     flops = FLOP_PER_PAIR * PAIRS / l1_mean_s / 1e12
     roof = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
             "traffic": _profiled_traffic() if args.config == "c2" else None,
-            "kernel": "gjx::l1_step_kernel<%s,%s,%d>" % ("true" if ALG & 1 else "false", "true" if ALG & 2 else "false",
-                                                      2 if 2 * PAIRS <= 148 else 1),
+            "kernel": "gjx::%s<%s,%s,%d>" % ("l1_sweep_kernel" if one_launch else "l1_step_kernel",
+                                             "true" if ALG & 1 else "false", "true" if ALG & 2 else "false",
+                                             2 if 2 * PAIRS <= 148 else 1),
             "peak_kind": f"{peak_kind} HBM copy bandwidth",
+            "per": ("outer step: a sweep launch's event time over its outer steps" if one_launch
+                    else "outer-step launch, event time"),
             "launch_ms": l1_mean_s * 1000.0, "launches": prof["l1_launches"],
             "algorithmic_bytes_per_launch": BYTES_PER_PAIR * PAIRS,
             "algorithmic_flop_per_launch": FLOP_PER_PAIR * PAIRS, "fp64_tflops": flops,
