@@ -460,8 +460,8 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
     if (steps > max_steps)
       max_steps = steps;
   }
-  // the work of each step index: block pairs of the matrices that have it,
-  // the largest matrices first (fewest stragglers at the end of a launch)
+  // the work of a launch: every block pair of every matrix, the largest
+  // matrices first (fewest stragglers at the end of a launch)
   std::vector<unsigned> order;
   for (unsigned b = 0u; b < nmat; ++b)
     if (ok[b])
@@ -469,25 +469,20 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
   std::stable_sort(order.begin(), order.end(), [&](unsigned x, unsigned y) {
     return (unsigned long long)nrow[x] * ncol[x] > (unsigned long long)nrow[y] * ncol[y];
   });
-  std::vector<uint32_t> items;
-  std::vector<unsigned> off(max_steps + 1u, 0u);
-  for (unsigned s = 0u; s < max_steps; ++s) {
-    off[s] = (unsigned)items.size();
-    for (unsigned b : order)
-      if (s < mats[b].steps1)
-        for (unsigned q = 0u; q < mats[b].p.pairs; ++q)
-          items.push_back((b << 16u) | q);
-  }
-  off[max_steps] = (unsigned)items.size();
   if (order.empty())
     return 0;
+  std::vector<uint32_t> items;
+  for (unsigned b : order)
+    for (unsigned q = 0u; q < mats[b].p.pairs; ++q)
+      items.push_back((b << 16u) | q);
 
   // device memory of the batch, one allocation
   auto up = [](size_t x) { return (x + 255u) & ~(size_t)255u; };
   const size_t o_mats = 0u, o_cvg = up(o_mats + nmat * sizeof(gjx::BatchMat)), o_done = up(o_cvg + nmat * 8u),
                o_ok = up(o_done + nmat * 4u), o_swp = up(o_ok + nmat * 4u), o_gs = up(o_swp + nmat * 4u),
-               o_gb = up(o_gs + nmat * 8u), o_q = up(o_gb + nmat * 8u), o_act = up(o_q + max_steps * 4u),
-               o_err = up(o_act + 4u), o_items = up(o_err + 8u), total = up(o_items + items.size() * 4u);
+               o_gb = up(o_gs + nmat * 8u), o_ks = up(o_gb + nmat * 8u), o_q = up(o_ks + nmat * 4u),
+               o_act = up(o_q + 4u), o_err = up(o_act + 4u), o_items = up(o_err + 8u),
+               total = up(o_items + items.size() * 4u);
   char *mem = nullptr;
   GJX_CUDA(cudaMalloc(&mem, total), "cudaMalloc(batch)");
   struct Free {
@@ -501,6 +496,7 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
   auto *d_swp = reinterpret_cast<unsigned *>(mem + o_swp);
   auto *d_gs = reinterpret_cast<unsigned long long *>(mem + o_gs);
   auto *d_gb = reinterpret_cast<unsigned long long *>(mem + o_gb);
+  auto *d_ks = reinterpret_cast<unsigned *>(mem + o_ks);
   auto *d_q = reinterpret_cast<unsigned *>(mem + o_q);
   auto *d_act = reinterpret_cast<unsigned *>(mem + o_act);
   auto *d_err = reinterpret_cast<int *>(mem + o_err);
@@ -527,23 +523,24 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
   GJX_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
   GJX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
 
-  // one sweep, captured once
+  // kLaunches launches (each followed by its step end), captured once
+  constexpr unsigned kLaunches = 8u;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   GJX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
   cudaError_t ce = cudaSuccess;
-  for (unsigned s = 0u; s < max_steps && ce == cudaSuccess; ++s) {
-    gjx::BatchStep bs{d_mats, d_items + off[s], off[s + 1u] - off[s], s, d_q, d_done, d_err};
-    const unsigned ctas = std::min<unsigned>((unsigned)sms, bs.nitems);
+  const gjx::BatchStep bs{d_mats, d_items, (unsigned)items.size(), d_ks, d_q, d_done, d_err};
+  const gjx::BatchSweep sw{d_mats, d_ks, d_cvg, d_done, d_swp, d_gs, d_gb, d_q, d_act, nmat};
+  const unsigned ctas = std::min<unsigned>((unsigned)sms, (unsigned)items.size());
+  for (unsigned k = 0u; k < kLaunches && ce == cudaSuccess; ++k) {
     ce = gjx::launch_batch_step(cdsort, full, bs, ctas, st);
+    if (ce == cudaSuccess)
+      ce = cudaMemsetAsync(d_act, 0, 4u, st); // the count of the last launch is the one read
+    if (ce == cudaSuccess)
+      ce = gjx::launch_batch_sweep_end(sw, st);
   }
-  if (ce == cudaSuccess)
-    ce = cudaMemsetAsync(d_act, 0, 4u, st);
-  gjx::BatchSweep sw{d_cvg, d_done, d_swp, d_gs, d_gb, d_q, d_act, nmat, max_steps};
-  if (ce == cudaSuccess)
-    ce = gjx::launch_batch_sweep_end(sw, st);
   const cudaError_t ee = cudaStreamEndCapture(st, &graph);
-  GJX_CUDA(ce, "capture of a batch sweep");
+  GJX_CUDA(ce, "capture of batch launches");
   GJX_CUDA(ee, "end capture");
   struct Graph {
     cudaGraph_t g;
@@ -558,15 +555,16 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
   } guard{graph, &exec};
   GJX_CUDA(cudaGraphInstantiate(&exec, graph, 0ull), "graph instantiate");
 
+  const unsigned max_replays = (gjx::kNSweep * max_steps + kLaunches - 1u) / kLaunches + 1u;
   unsigned active = 0u;
   int err = 0;
-  for (unsigned k = 0u; k < gjx::kNSweep; ++k) {
+  for (unsigned k = 0u; k < max_replays; ++k) {
     GJX_CUDA(cudaGraphLaunch(exec, st), "graph launch");
-    g_prof.launches += max_steps + 1u;
-    g_prof.l1_launches += max_steps;
+    g_prof.launches += 2u * kLaunches;
+    g_prof.l1_launches += kLaunches;
     GJX_CUDA(cudaMemcpyAsync(&active, d_act, 4u, cudaMemcpyDeviceToHost, st), "read batch state");
     GJX_CUDA(cudaMemcpyAsync(&err, d_err, 4u, cudaMemcpyDeviceToHost, st), "read batch state");
-    GJX_CUDA(cudaStreamSynchronize(st), "batch sweep");
+    GJX_CUDA(cudaStreamSynchronize(st), "batch launches");
     if (err) {
       g_err = "a block-pair kernel timed out waiting for its tile copies";
       return GJX_ERR_DEVICE;

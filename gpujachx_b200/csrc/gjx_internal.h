@@ -40,25 +40,30 @@ struct alignas(64) BatchMat {
   unsigned steps1; // outer steps per sweep of this matrix
 };
 
-// one outer-step launch of a batch
+// one launch of a batch: every active matrix advances by one outer step of
+// its own sweep (matrix b is at step kstep[b] mod steps1 of its sweep)
 struct BatchStep {
   const BatchMat *mats;
-  const uint32_t *items; // (matrix << 16) | pair of this step, largest matrices first
-  unsigned nitems, step;
-  unsigned *queue;       // work-queue heads, one per step index
-  const uint32_t *done;  // converged or failed matrices (skipped)
-  const int *err;        // any nonzero: stop
+  const uint32_t *items;   // (matrix << 16) | pair of every matrix, largest matrices first
+  unsigned nitems;
+  const unsigned *kstep;   // per matrix: outer steps done so far
+  unsigned *queue;         // work-queue head (cleared by the step end)
+  const uint32_t *done;    // converged or failed matrices (skipped)
+  const int *err;          // any nonzero: stop
 };
 
-// end-of-sweep bookkeeping of a batch
+// after each launch: per matrix, count the step; at the end of its sweep fold
+// the sweep's counter into its totals and test convergence
 struct BatchSweep {
-  unsigned long long *cvg; // per matrix, (big << 32) | small of the sweep
+  const BatchMat *mats;
+  unsigned *kstep;
+  unsigned long long *cvg; // per matrix, (big << 32) | small of the current sweep
   uint32_t *done;
   unsigned *sweeps;
   unsigned long long *glb_s, *glb_b;
   unsigned *queue;
-  unsigned *active; // matrices still sweeping after this sweep
-  unsigned nmat, nqueue;
+  unsigned *active; // matrices still sweeping (accumulated; cleared by the host between checks)
+  unsigned nmat;
 };
 
 cudaError_t batch_configure();

@@ -808,13 +808,15 @@ __global__ void __launch_bounds__(kThreads, 1) l1_sweep_kernel(const __grid_cons
 }
 
 // ---------------------------------------------------------------------------
-// Batched form: one launch per outer step index for a whole batch of
-// independent matrices.  A persistent grid (one CTA per SM) takes the step's
-// block pairs -- (matrix << 16) | pair, largest matrices first -- from a
-// work queue; each is processed by pair_step exactly as in the single-matrix
-// launch with one CTA per pair, so every matrix gets the bits it would get
-// alone.  Matrices already converged are skipped.  The mbarriers are
-// invalidated after each pair (pair_step initialises them).
+// Batched form: each launch advances every active matrix of a batch by one
+// outer step of its own sweep (matrix b: step kstep[b] mod steps1), so small
+// matrices run their short sweeps back to back while large ones progress.  A
+// persistent grid (one CTA per SM) takes the block pairs -- (matrix << 16) |
+// pair, largest matrices first -- from a work queue; each is processed by
+// pair_step exactly as in the single-matrix launch with one CTA per pair, so
+// every matrix gets the bits it would get alone.  Converged matrices are
+// skipped.  The mbarriers are invalidated after each pair (pair_step
+// initialises them).
 // ---------------------------------------------------------------------------
 template <bool SORT, bool ACCV>
 __global__ void __launch_bounds__(kThreads, 1) l1_batch_kernel(const __grid_constant__ BatchStep B)
@@ -824,7 +826,7 @@ __global__ void __launch_bounds__(kThreads, 1) l1_batch_kernel(const __grid_cons
   uint64_t *const bars = reinterpret_cast<uint64_t *>(sm + kOffBar);
   for (;;) {
     if (threadIdx.x == 0u)
-      item = atomicAdd(B.queue + B.step, 1u);
+      item = atomicAdd(B.queue, 1u);
     __syncthreads();
     const unsigned it = item;
     const bool stop = (it >= B.nitems) || (*(volatile int *)B.err != 0);
@@ -835,7 +837,8 @@ __global__ void __launch_bounds__(kThreads, 1) l1_batch_kernel(const __grid_cons
     const unsigned b = e >> 16u, pair = e & 0xffffu;
     if (B.done[b])
       continue;
-    pair_step<SORT, ACCV, 1u>(B.mats[b].p, B.step, pair, 0u, sm);
+    const BatchMat &m = B.mats[b];
+    pair_step<SORT, ACCV, 1u>(m.p, B.kstep[b] % m.steps1, pair, 0u, sm);
     __syncthreads();
     if (threadIdx.x == 0u)
       for (unsigned k = 0u; k < 8u; ++k)
@@ -844,15 +847,21 @@ __global__ void __launch_bounds__(kThreads, 1) l1_batch_kernel(const __grid_cons
   }
 }
 
-// end of a sweep of the batch: per-matrix totals, convergence (no big
-// rotation in the sweep, or the sweep cap), the next sweep's queues cleared
+// after a launch of the batch: one step more for every active matrix; at the
+// end of its sweep, its totals and the convergence test (no big rotation in
+// the sweep, or the sweep cap); the work queue cleared for the next launch
 __global__ void batch_sweep_end_kernel(const BatchSweep S)
 {
   const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < S.nqueue)
-    S.queue[i] = 0u;
+  if (i == 0u)
+    S.queue[0] = 0u;
   if (i >= S.nmat || S.done[i])
     return;
+  const unsigned k = ++S.kstep[i];
+  if (k % S.mats[i].steps1) { // the sweep goes on
+    atomicAdd(S.active, 1u);
+    return;
+  }
   const unsigned long long c = S.cvg[i];
   S.cvg[i] = 0ull;
   const unsigned small = (unsigned)c, big = (unsigned)(c >> 32u);
@@ -1039,8 +1048,7 @@ cudaError_t launch_batch_step(const bool sort, const bool accv, const BatchStep 
 
 cudaError_t launch_batch_sweep_end(const BatchSweep &w, cudaStream_t s)
 {
-  const unsigned n = (w.nmat > w.nqueue) ? w.nmat : w.nqueue;
-  batch_sweep_end_kernel<<<(n + 255u) / 256u, 256u, 0, s>>>(w);
+  batch_sweep_end_kernel<<<(w.nmat + 255u) / 256u, 256u, 0, s>>>(w);
   return cudaGetLastError();
 }
 
