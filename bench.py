@@ -592,6 +592,8 @@ def main():
             dist.barrier()
 
     g.init_strats(None, "cycwor", 32, "cycwor", N1)
+    if os.environ.get("GJX_SWEEP_MODE") == "0":  # one launch per outer step (profilers cannot replay the sweep launch)
+        g.lib().gjx_set_sweep_mode(0)
     G0 = _input()
     dev = torch.device("cuda", local)
     # device layout: row j of the (N, M) tensor = column j of G
