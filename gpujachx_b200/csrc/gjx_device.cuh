@@ -247,4 +247,13 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *tm, co
                : "memory");
 }
 
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *tm, const int c0, const int c1,
+                                            const int c2, const int c3, uint64_t *bar)
+{
+  asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+               "%5}], [%6];" ::"r"(smem_u32(dst)),
+               "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+               : "memory");
+}
+
 } // namespace gjx

@@ -210,6 +210,7 @@ int run_sweeps_core(const unsigned routine, const unsigned nrow, const unsigned 
   p.gdefinite = (nplus ? ((nplus < ncol) ? 0 : +1) : -1);
   p.split = gjx::l1_split(p.pairs);
   GJX_CUDA(gjx::make_update_map(&p.tmG, dG, nrow, ncol, lddG), "tensor map of G");
+  GJX_CUDA(gjx::make_gram_map(&p.tmGram, dG, nrow, ncol, lddG), "Gram tensor map of G");
   if (full)
     GJX_CUDA(gjx::make_update_map(&p.tmV, dV, ncol, ncol, lddV), "tensor map of V");
 
@@ -452,6 +453,7 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
     p.gdefinite = (nplus[b] ? ((nplus[b] < ncol[b]) ? 0 : +1) : -1);
     p.split = 1u;
     GJX_CUDA(gjx::make_update_map(&p.tmG, dG[b], nrow[b], ncol[b], lddG[b]), "tensor map of G");
+    GJX_CUDA(gjx::make_gram_map(&p.tmGram, dG[b], nrow[b], ncol[b], lddG[b]), "Gram tensor map of G");
     if (full)
       GJX_CUDA(gjx::make_update_map(&p.tmV, dV[b], ncol[b], ncol[b], lddV[b]), "tensor map of V");
     mats[b].D = dD[b];

@@ -16,6 +16,7 @@ constexpr unsigned kNSweep = 30u; // outer and full-block inner sweep cap (share
 struct alignas(64) StepParams {
   CUtensorMap tmG;              // 3-D view (32 rows, nrow/32 pieces, ncol columns) of G
   CUtensorMap tmV;              // the same of V (ACCV only)
+  CUtensorMap tmGram;           // 4-D view (32 rows, 2 pieces, nrow/64 tiles, ncol columns) of G
   double *G;                    // nrow x ncol, column major, leading dim ldG
   double *V;                    // ncol x ncol, leading dim ldV (ACCV only)
   const uint16_t *strat1;       // [steps1][pairs][2] block pairs (outer level)
@@ -78,6 +79,8 @@ cudaError_t launch_batch_initD(const BatchMat *m, unsigned nmat, const uint32_t 
 
 // TMA tensor maps for the update staging (3-D view, box {34, 8, 16}); 0 or a CUDA error
 cudaError_t make_update_map(CUtensorMap *tm, const double *base, unsigned nrow, unsigned ncol, unsigned ld);
+// TMA tensor map for the Gram staging (4-D view, box {34, 3, 1, 16})
+cudaError_t make_gram_map(CUtensorMap *tm, const double *base, unsigned nrow, unsigned ncol, unsigned ld);
 
 // device error codes written to *err
 enum : int { kErrWaitTimeout = 1 };

@@ -47,21 +47,21 @@ namespace gjx {
 constexpr unsigned kThreads = 256u;
 constexpr long long kWaitLimit = 2000000000ll; // ~1 s of cycles per wait
 
-// Gram staging: a stage holds 2 tiles of 64 rows of the 32 columns; tile t
-// of column c at gcol_off(c) + 96 t, rows 0..95 where rows 64..95 repeat
-// rows 0..31, so a chain starting at tile row x reads rows x..x+63 without
-// wrapping.  Filled by 16-byte cp.async (the layout needs 16-byte placement
-// freedom: repeated rows and per-column bank offsets), 3 stages in flight.
-// The offset of column c, 2 ((c + c/8) mod 8) doubles, puts the 16-byte row
-// pairs of 8 consecutive columns in 8 different bank groups (the column
-// stride is 0 mod 16 doubles), and keeps apart the two columns x0 + u that
-// a warp with two x-blocks reads at once.
+// Gram staging: a stage holds 2 tiles of 64 rows of the 32 columns, brought
+// in by the TMA engine: per tile and block one box {34 rows, 3 pieces, 1 tile,
+// 16 columns} of the 4-D view (32 rows, 2 pieces, tiles, columns) of G.  Rows
+// 32-33 of a piece and the third piece lie outside the view and are
+// zero-filled, so column c of a tile starts at c * 102 and tile row r sits at
+// r + 2 (r >> 5).  The column stride of 102 doubles (51 16-byte granules, odd)
+// puts the row pairs of 8 consecutive columns in 8 bank groups.  3 stages in
+// flight.
 constexpr unsigned kGramTiles = 2u;
 constexpr unsigned kGramStages = 3u;
-constexpr unsigned kGramColLd = 2u * 96u + 16u;
-constexpr unsigned kGramStage = 32u * kGramColLd; // doubles
-constexpr unsigned kGramChunks = 48u;             // 16-byte chunks per column and tile
-__device__ __forceinline__ unsigned gcol_off(const unsigned c) { return c * kGramColLd + 2u * ((c + (c >> 3)) & 7u); }
+constexpr unsigned kGramColLd = 102u;
+constexpr unsigned kGramTileLd = 32u * kGramColLd;
+constexpr unsigned kGramStage = kGramTiles * kGramTileLd; // doubles
+constexpr uint32_t kGramBoxBytes = 34u * 3u * 16u * 8u;
+__device__ __forceinline__ unsigned grow(const unsigned r) { return r + 2u * (r >> 5); }
 
 // Update staging: 256 rows x 32 columns; the 32-row piece p of column c
 // starts at c*272 + p*34 (2 doubles of skew per piece spread the banks).
@@ -98,39 +98,38 @@ size_t l1_smem_bytes() { return (size_t)kSmemDoubles * sizeof(double); }
 #define E32(A, r, c) (A)[(c) * 32u + (r)]
 
 // ---------------------------------------------------------------------------
-// Gram: one 64-row tile (at row base of the stage) for the 4 entries
+// Gram: one 64-row tile (at offset base of the stage) for the 4 entries
 // (x0+u, y), u < 4, of one lane.  Entry (x, y) adds G[r,y]*G[r,x] for
 // r = x, x+1, ..., x+63 (mod 64), the reference's order.  With k = r - x0
-// (0..66; rows 64..95 of a tile repeat rows 0..31) chain u takes the k in
-// [u, u+63] in increasing order.  Operands come in 16-byte pairs of rows
-// (k, k+1), k even: one pair of column y and one of each column x0+u per
+// (0..66, taken mod 64) chain u takes the k in [u, u+63] in increasing order.
+// Operands come in 16-byte pairs of rows (k, k+1), k even (a pair never
+// straddles a piece): one pair of column y and one of each column x0+u per
 // two rows; the pairs of k + 4 are in flight while those of k are used.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void gram_tile(const double *const st, const unsigned base, const unsigned x0,
                                           const unsigned y, double (&acc)[4])
 {
-  const double *const yp = st + gcol_off(y) + base + x0;
-  const double *xp[4];
-#pragma unroll
-  for (unsigned u = 0u; u < 4u; ++u)
-    xp[u] = st + gcol_off(x0 + u) + base + x0;
+  const double *const yp = st + base + y * kGramColLd;
+  const double *const xp = st + base + x0 * kGramColLd;
   double2 Yb[3], Xb[3][4];
 #pragma unroll
   for (unsigned q = 0u; q < 2u; ++q) {
-    Yb[q] = *reinterpret_cast<const double2 *>(yp + 2u * q);
+    const unsigned o = grow((x0 + 2u * q) & 63u);
+    Yb[q] = *reinterpret_cast<const double2 *>(yp + o);
 #pragma unroll
     for (unsigned u = 0u; u < 4u; ++u)
-      Xb[q][u] = *reinterpret_cast<const double2 *>(xp[u] + 2u * q);
+      Xb[q][u] = *reinterpret_cast<const double2 *>(xp + u * kGramColLd + o);
   }
 #pragma unroll
   for (unsigned kp = 0u; kp < 34u; ++kp) { // pairs k = 2kp, 2kp + 1
     if (kp + 2u < 34u) {
       const unsigned q = (kp + 2u) % 3u;
-      Yb[q] = *reinterpret_cast<const double2 *>(yp + 2u * (kp + 2u));
+      const unsigned o = grow((x0 + 2u * (kp + 2u)) & 63u);
+      Yb[q] = *reinterpret_cast<const double2 *>(yp + o);
 #pragma unroll
       for (unsigned u = 0u; u < 4u; ++u)
         if (2u * (kp + 2u) + 1u >= u && 2u * (kp + 2u) <= u + 63u)
-          Xb[q][u] = *reinterpret_cast<const double2 *>(xp[u] + 2u * (kp + 2u));
+          Xb[q][u] = *reinterpret_cast<const double2 *>(xp + u * kGramColLd + o);
     }
     const unsigned q = kp % 3u;
 #pragma unroll
@@ -493,7 +492,7 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
     reinterpret_cast<uint32_t *>(s0)[i] = reinterpret_cast<const uint32_t *>(P.strat0)[i];
   if (tid == 0u) {
     for (unsigned b = 0u; b < 8u; ++b)
-      mbar_init(&bars[b], (b < kGramStages) ? ((NSPLIT > 1u) ? kThreads / 2u : kThreads) : 1u);
+      mbar_init(&bars[b], 1u); // one arrival with the expected bytes, the TMA engine completes it
     mbar_fence_init();
   }
   __syncthreads();
@@ -506,40 +505,27 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
   double gacc[4] = {+0.0, +0.0, +0.0, +0.0};
 
   const unsigned ngst = (ntile + kGramTiles - 1u) / kGramTiles; // stages of 2 tiles
-  // all threads: 16-byte cp.async of stage k (each column: per tile 32 chunks
-  // of rows 0..63 and 16 chunks repeating rows 0..31), then one arrival on the
-  // stage's mbarrier when this thread's copies have landed
-  // copy producers: in a 2-CTA cluster the 4 warps that compute no Gram
-  // entries (each thread 2 columns' share), else all 8 warps (1 column each);
-  // a column's 48 chunks per tile are spread over its threads in steps of the
-  // thread count per column, rows 0..63 first, then the repeat of rows 0..31
-  const unsigned nprod = (NSPLIT > 1u) ? kThreads / 2u : kThreads;
-  const bool producer = (NSPLIT > 1u) ? (warp >= 4u) : true;
-  const unsigned ptid = (NSPLIT > 1u) ? (tid - kThreads / 2u) : tid;
-  const unsigned tpc = nprod / 32u;                   // threads per column
-  const unsigned pcol = ptid / tpc, psub = ptid % tpc; // this thread's column and offset
-  const double *const pcolp = (pcol < 16u) ? (Gi + (size_t)pcol * P.ldG) : (Gj + (size_t)(pcol - 16u) * P.ldG);
+  // thread 0: the TMA engine brings stage k, per tile block i's and block j's
+  // 16 columns as one box each
   auto issue_gram = [&](const unsigned k) {
     const unsigned s = k % kGramStages;
     const unsigned nt = min(kGramTiles, ntile - k * kGramTiles);
-    double *const dcol = stg + s * kGramStage + gcol_off(pcol);
+    double *const st = stg + s * kGramStage;
+    mbar_arrive_expect_tx(&bars[s], nt * 2u * kGramBoxBytes);
     for (unsigned t = 0u; t < nt; ++t) {
-      const double *const src = pcolp + (size_t)(k * kGramTiles + t) * 64u;
-      for (unsigned q = psub; q < kGramChunks; q += tpc) {
-        const unsigned srow = (q < 32u) ? 2u * q : 2u * q - 64u;
-        cp_async16(dcol + t * 96u + 2u * q, src + srow);
-      }
+      const int tile = (int)(k * kGramTiles + t);
+      tma_load_4d(st + t * kGramTileLd, &P.tmGram, 0, 0, tile, (int)(iBlk * kNColB), &bars[s]);
+      tma_load_4d(st + t * kGramTileLd + 16u * kGramColLd, &P.tmGram, 0, 0, tile, (int)(jBlk * kNColB), &bars[s]);
     }
-    cp_async_arrive(&bars[s]);
   };
 
-  if (producer)
+  if (tid == 0u)
     for (unsigned k = 0u; k + 1u < kGramStages && k < ngst; ++k)
       issue_gram(k);
   unsigned k = 0u;
   int failed = 0;
   for (; k < ngst; ++k) {
-    if (producer && k + kGramStages - 1u < ngst)
+    if (tid == 0u && k + kGramStages - 1u < ngst)
       issue_gram(k + kGramStages - 1u); // into the buffer released at the end of stage k - 1
     int fail = 0;
     if (warp < gwarps) {
@@ -548,17 +534,17 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
       else if (gthr) {
         const unsigned nt = min(kGramTiles, ntile - k * kGramTiles);
         for (unsigned t = 0u; t < nt; ++t)
-          gram_tile(stg + (k % kGramStages) * kGramStage, t * 96u, gx0, gy, gacc);
+          gram_tile(stg + (k % kGramStages) * kGramStage, t * kGramTileLd, gx0, gy, gacc);
       }
     }
     failed = __syncthreads_or(fail); // uniform decision
     if (failed)
       break;
   }
-  if (failed) { // let this thread's copies land before anything else, report
-    cp_async_wait_all();
-    if (tid == 0u)
-      atomicOr(P.err, kErrWaitTimeout);
+  if (failed && tid == 0u) { // let the copies in flight land (bounded) before anything else, report
+    for (unsigned q = k; q < ngst && q < k + kGramStages; ++q)
+      (void)mbar_wait_bounded(&bars[q % kGramStages], (q / kGramStages) & 1u, kWaitLimit / 8);
+    atomicOr(P.err, kErrWaitTimeout);
   }
   // our share of the lower triangle, into our R and the other CTAs' R
   if (gthr) {
@@ -976,6 +962,31 @@ cudaError_t make_update_map(CUtensorMap *tm, const double *base, const unsigned 
   const cuuint32_t box[3] = {34u, 8u, 16u};
   const cuuint32_t estr[3] = {1u, 1u, 1u};
   const CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3u, const_cast<double *>(base), dims, strides, box,
+                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return (r == CUDA_SUCCESS) ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+cudaError_t make_gram_map(CUtensorMap *tm, const double *base, const unsigned nrow, const unsigned ncol,
+                          const unsigned ld)
+{
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess)
+      return e;
+    if (q != cudaDriverEntryPointSuccess || !fn)
+      return cudaErrorNotSupported;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  // (rows within a 32-row piece, 2 pieces, 64-row tiles, columns); box {34, 3, 1, 16}
+  const cuuint64_t dims[4] = {32u, 2u, nrow / 64u, ncol};
+  const cuuint64_t strides[3] = {32u * sizeof(double), 64u * sizeof(double), (cuuint64_t)ld * sizeof(double)};
+  const cuuint32_t box[4] = {34u, 3u, 1u, 16u};
+  const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
+  const CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4u, const_cast<double *>(base), dims, strides, box,
                             estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return (r == CUDA_SUCCESS) ? cudaSuccess : cudaErrorInvalidValue;
