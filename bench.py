@@ -594,6 +594,7 @@ def main():
     g.init_strats(None, "cycwor", 32, "cycwor", N1)
     if os.environ.get("GJX_SWEEP_MODE") == "0":  # one launch per outer step (profilers cannot replay the sweep launch)
         g.lib().gjx_set_sweep_mode(0)
+    tuned = g.autotune(ALG, M, N, NPLUS, sweeps=1)  # the library's autotuner, once per shape, before timing
     G0 = _input()
     dev = torch.device("cuda", local)
     # device layout: row j of the (N, M) tensor = column j of G
@@ -644,7 +645,7 @@ def main():
             "traffic": _profiled_traffic() if args.config == "c2" else None,
             "kernel": "gjx::%s<%s,%s,%d>" % ("l1_sweep_kernel" if one_launch else "l1_step_kernel",
                                              "true" if ALG & 1 else "false", "true" if ALG & 2 else "false",
-                                             2 if 2 * PAIRS <= 148 else 1),
+                                             tuned["split"]),
             "peak_kind": f"{peak_kind} HBM copy bandwidth",
             "per": ("outer step: a sweep launch's event time over its outer steps" if one_launch
                     else "outer-step launch, event time"),
@@ -683,6 +684,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(CONFIG, parallelism=("replicas" if world > 1 else "single GPU")),
             "sweeps": sweeps, "e2e": e2e, "roofline": roof, "clocks": clk,
+            "tuned": {"ctas_per_pair": tuned["split"], "one_launch_per_sweep": bool(tuned["mode"])},
             "gpu_launches": prof["launches"], "step_ms": times}
     if rank == 0 and args.accuracy:
         line["accuracy"] = accuracy_figures(G0, dG.cpu().numpy().T, dV.cpu().numpy().T if ALG & 2 else None,

@@ -35,7 +35,8 @@ EXPORTS = ("hypJacL2", "init_strats", "gjx_init_strats", "gjx_strat_info", "gjx_
            "gjx_hypJacL2_dev", "gjx_release_cache", "gjx_set_verbose", "gjx_last_error",
            "gjx_version", "gjx_rsqrt_rn_dev", "gjx_profile", "gjx_profile_read", "gjx_hypJacL2_noalloc",
            "gjx_validate_pairs", "gjx_validate_strats", "gjx_configure_device", "gjx_h5_read", "gjx_h5_write",
-           "gjx_hypJacL2_batched", "gjx_set_sweep_mode")
+           "gjx_hypJacL2_batched", "gjx_set_sweep_mode", "gjx_set_split", "gjx_autotune",
+           "gjx_autotune_clear")
 
 
 class GjxError(RuntimeError):
@@ -96,6 +97,12 @@ def lib() -> ctypes.CDLL:
     L.gjx_hypJacL2_batched.argtypes = [u, u, pu, pu, pu, pp, pu, pp, pu, pp, ctypes.c_void_p, pu, pull, pull,
                                        ctypes.POINTER(ctypes.c_int)]
     L.gjx_hypJacL2_batched.restype = i
+    L.gjx_autotune.argtypes = [u, u, u, u, u, pu]
+    L.gjx_autotune.restype = i
+    L.gjx_autotune_clear.argtypes = []
+    L.gjx_autotune_clear.restype = None
+    L.gjx_set_split.argtypes = [u]
+    L.gjx_set_split.restype = None
     L.gjx_set_sweep_mode.argtypes = [i]
     L.gjx_set_sweep_mode.restype = None
     L.gjx_configure_device.argtypes = [i]
@@ -273,4 +280,14 @@ def hypJacL2_batched(routine: int, Gs, nplus, Vs=None, Ds=None, stream=None, nro
     if ret:
         raise GjxError(ret, last_error())
     return BatchResult(ret, list(info), list(sw), list(rs), list(rb))
+
+
+def autotune(routine: int, nrow: int, ncol: int, nplus: int, sweeps: int = 1) -> dict:
+    """Time the launch configurations of this shape and keep the fastest for
+    later calls (gjx_autotune); returns {"split": CTAs per pair, "mode": 0/1}."""
+    out = (ctypes.c_uint * 2)()
+    r = lib().gjx_autotune(routine, nrow, ncol, nplus, sweeps, out)
+    if r:
+        raise GjxError(r, last_error() if r > 0 else "invalid argument")
+    return {"split": out[0], "mode": out[1]}
 

@@ -21,7 +21,9 @@
 #include <cstring>
 #include <algorithm>
 #include <dlfcn.h>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -46,7 +48,19 @@ struct Strat {
 std::mutex g_mtx;
 Strat g_strat;
 int g_verbose = 1;
-int g_sweep_mode = 1; // 1: one launch per sweep where every cluster fits; 0: one launch per outer step
+int g_sweep_mode = -1; // -1 automatic (the tuned choice, else per step), 0 per outer step, 1 one launch per sweep
+unsigned g_split = 0u;  // CTAs per block pair: 0 automatic (the tuned choice, else by the SM count), else 1, 2, 4
+
+// the autotuner's choices, by (routine, nrow, ncol, nplus)
+struct TuneKey {
+  unsigned routine, nrow, ncol, nplus;
+  bool operator<(const TuneKey &o) const
+  {
+    return std::tie(routine, nrow, ncol, nplus) < std::tie(o.routine, o.nrow, o.ncol, o.nplus);
+  }
+};
+std::map<TuneKey, std::pair<unsigned, int>> g_tuned; // (split, sweep mode)
+unsigned g_sweep_cap = 0u; // nonzero: stop after this many sweeps (the autotuner's timed runs)
 
 // profiling: launch counts always; with g_prof, CUDA events around every
 // block-pair launch, read back at the end of each sweep
@@ -209,6 +223,16 @@ int run_sweeps_core(const unsigned routine, const unsigned nrow, const unsigned 
   p.nswp0 = blk_ori ? 1u : gjx::kNSweep;
   p.gdefinite = (nplus ? ((nplus < ncol) ? 0 : +1) : -1);
   p.split = gjx::l1_split(p.pairs);
+  int mode = g_sweep_mode;
+  const auto tuned = g_tuned.find(TuneKey{routine, nrow, ncol, nplus});
+  if (tuned != g_tuned.end()) {
+    if (!g_split)
+      p.split = tuned->second.first;
+    if (mode < 0)
+      mode = tuned->second.second;
+  }
+  if (g_split && g_split * p.pairs <= 148u * 8u)
+    p.split = g_split;
   GJX_CUDA(gjx::make_update_map(&p.tmG, dG, nrow, ncol, lddG), "tensor map of G");
   GJX_CUDA(gjx::make_gram_map(&p.tmGram, dG, nrow, ncol, lddG), "Gram tensor map of G");
   if (full)
@@ -222,8 +246,9 @@ int run_sweeps_core(const unsigned routine, const unsigned nrow, const unsigned 
   p.steps1 = g_strat.steps1;
   p.ver = d_ver;
   // one launch per sweep when all clusters of a step are resident together
-  bool one_launch = d_ver && g_sweep_mode && g_strat.n1 <= 1024u && gjx::sweep_kernel_fits(cdsort, full, p);
-  while (blk_swp < gjx::kNSweep) {
+  bool one_launch = d_ver && mode > 0 && g_strat.n1 <= 1024u && gjx::sweep_kernel_fits(cdsort, full, p);
+  const unsigned cap = g_sweep_cap ? g_sweep_cap : gjx::kNSweep;
+  while (blk_swp < cap) {
     GJX_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st), "clear counter");
     if (one_launch) {
       GJX_CUDA(cudaMemsetAsync(d_ver, 0, g_strat.n1 * sizeof(unsigned), st), "clear block counts");
@@ -1041,7 +1066,105 @@ int gjx_hypJacL2_batched(const unsigned routine, const unsigned nmat, const unsi
 void gjx_set_sweep_mode(const int mode)
 {
   std::lock_guard<std::mutex> lk(g_mtx);
-  g_sweep_mode = mode ? 1 : 0;
+  g_sweep_mode = (mode < 0) ? -1 : (mode ? 1 : 0);
+}
+
+void gjx_set_split(const unsigned n)
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  g_split = (n == 1u || n == 2u || n == 4u) ? n : 0u;
+}
+
+int gjx_autotune(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
+                 const unsigned sweeps, unsigned *const out)
+{
+  if (const int r = check_args(routine, nrow, ncol, nplus, reinterpret_cast<const double *>(16), nrow,
+                               reinterpret_cast<const double *>(16), ncol, reinterpret_cast<const double *>(16),
+                               reinterpret_cast<const unsigned *>(16), reinterpret_cast<const unsigned long long *>(16),
+                               reinterpret_cast<const unsigned long long *>(16)))
+    return r;
+  std::lock_guard<std::mutex> lk(g_mtx);
+  if (!g_strat.loaded)
+    return GJX_ERR_NO_STRAT;
+  if (ncol / gjx::kNColB != g_strat.n1)
+    return GJX_ERR_STRAT_ORDER;
+  DevCtx *ctx = nullptr;
+  if (const int r = dev_ctx(ctx))
+    return r;
+  if (const int r = upload_strat(*ctx, nullptr))
+    return r;
+  const bool full = (routine & GJX_FULL_SVD) != 0u;
+  const unsigned ld = nrow + (nrow & 1u);
+  double *mem = nullptr;
+  const size_t nG = (size_t)ld * ncol, nV = full ? (size_t)ncol * ncol : 0u;
+  GJX_CUDA(cudaMalloc(&mem, (2u * nG + nV + ncol) * sizeof(double)), "cudaMalloc(autotune)");
+  struct Free {
+    double *m;
+    ~Free() { (void)cudaFree(m); }
+  } fm{mem};
+  double *const g0 = mem, *const g = mem + nG, *const v = g + nG, *const d = v + nV;
+  GJX_CUDA(gjx::launch_fill_random(g0, nG, 0x5eed0000ull + ncol, nullptr), "autotune input");
+  cudaEvent_t e0, e1;
+  GJX_CUDA(cudaEventCreate(&e0), "cudaEventCreate");
+  GJX_CUDA(cudaEventCreate(&e1), "cudaEventCreate");
+  const int saved_mode = g_sweep_mode;
+  const unsigned saved_split = g_split, saved_cap = g_sweep_cap, saved_verbose = (unsigned)g_verbose;
+  g_verbose = 0;
+  g_sweep_cap = sweeps ? sweeps : 1u;
+  float best = 3.0e38f;
+  std::pair<unsigned, int> pick{gjx::l1_split(g_strat.pairs1), 0};
+  int rc = 0;
+  for (unsigned split : {1u, 2u, 4u}) {
+    if (split * g_strat.pairs1 > 148u * 8u)
+      continue;
+    for (int mode : {0, 1}) {
+      g_split = split;
+      g_sweep_mode = mode;
+      unsigned swp;
+      unsigned long long s_, b_;
+      float ms = 0.0f;
+      for (int rep = 0; rep < 2 && !rc; ++rep) { // the first run warms up
+        if (cudaMemcpyAsync(g, g0, nG * sizeof(double), cudaMemcpyDeviceToDevice, nullptr) != cudaSuccess ||
+            cudaEventRecord(e0, nullptr) != cudaSuccess) {
+          rc = GJX_ERR_CUDA;
+          break;
+        }
+        rc = run_sweeps_core(routine, nrow, ncol, nplus, g, ld, full ? v : nullptr, ncol, d, nullptr, ctx->d_s0,
+                             ctx->d_s1, ctx->d_cnt, ctx->h_cnt, ctx->d_ver, false, &swp, &s_, &b_);
+        if (!rc && (cudaEventRecord(e1, nullptr) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                    cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+          rc = GJX_ERR_CUDA;
+      }
+      if (rc)
+        break;
+      if (ms < best) {
+        best = ms;
+        pick = {split, mode};
+      }
+    }
+    if (rc)
+      break;
+  }
+  g_sweep_mode = saved_mode;
+  g_split = saved_split;
+  g_sweep_cap = saved_cap;
+  g_verbose = (int)saved_verbose;
+  (void)cudaEventDestroy(e0);
+  (void)cudaEventDestroy(e1);
+  if (rc)
+    return rc;
+  g_tuned[TuneKey{routine, nrow, ncol, nplus}] = pick;
+  if (out) {
+    out[0] = pick.first;
+    out[1] = (unsigned)pick.second;
+  }
+  return 0;
+}
+
+void gjx_autotune_clear(void)
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  g_tuned.clear();
 }
 
 } // extern "C"

@@ -1,8 +1,8 @@
 // gjx_kernels.cu -- sm_100a kernels of the blocked one-sided Jacobi (H)SVD.
 //
 // One block pair (i, j) of an outer step is processed by a cluster of NSPLIT
-// CTAs (NSPLIT = 2 when the step has few pairs, so that both SMs of a pair
-// work on it; 1 when the pairs already fill the GPU), 256 threads each:
+// CTAs (NSPLIT = 4 or 2 when the step has few pairs, so that more SMs work on
+// each pair; 1 when the pairs already fill the GPU), 256 threads each:
 //
 //   1. Gram matrix of the M x 32 column pair [G_i G_j], lower triangle only
 //      (the Cholesky never reads the upper one).  Each CTA streams the whole
@@ -150,12 +150,19 @@ __device__ __forceinline__ void gram_tile(const double *const st, const unsigned
 // lanes), so that the 4 operands of column x0+u are shared by the warp.
 //   one CTA:  warps 0..4 = (7), (6,0), (5,1), (4,2), (3)
 //   2-CTA cluster, rank 0: (7), (6,0), (1); rank 1: (5), (4,2), (3)
+//   4-CTA cluster, rank r: (7 - r), (r)
 template <unsigned NSPLIT>
 __device__ __forceinline__ bool gram_lane_of(const unsigned rank, const unsigned warp, const unsigned lane,
                                              unsigned &x0, unsigned &y)
 {
   int p, sb;
-  if (NSPLIT == 1u) { // (7), (6,0), (5,1), (4,2), (3)
+  if (NSPLIT == 4u) { // rank r: warps (7 - r), (r)
+    if (warp >= 2u)
+      return false;
+    p = (warp == 0u) ? 7 - (int)rank : (int)rank;
+    sb = -1;
+  }
+  else if (NSPLIT == 1u) { // (7), (6,0), (5,1), (4,2), (3)
     if (warp >= 5u)
       return false;
     p = 7 - (int)warp;
@@ -500,7 +507,7 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
   // ------------------------------ 1. Gram --------------------------------
   const unsigned ntile = P.nrow >> 6; // 64-row tiles
   unsigned gx0 = 0u, gy = 0u;
-  const unsigned gwarps = (NSPLIT > 1u) ? 3u : 5u;
+  const unsigned gwarps = (NSPLIT == 4u) ? 2u : (NSPLIT == 2u) ? 3u : 5u;
   const bool gthr = gram_lane_of<NSPLIT>(rank, warp, lane, gx0, gy);
   double gacc[4] = {+0.0, +0.0, +0.0, +0.0};
 
@@ -747,7 +754,7 @@ template <bool SORT, bool ACCV, unsigned NSPLIT>
 __global__ void __launch_bounds__(kThreads, 1) l1_sweep_kernel(const __grid_constant__ StepParams P)
 {
   extern __shared__ __align__(128) double sm[];
-  __shared__ unsigned agree[2]; // [0] this CTA may proceed, [1] the peer CTA may
+  __shared__ unsigned agree[NSPLIT]; // [r]: CTA r of the cluster may proceed
   uint64_t *const bars = reinterpret_cast<uint64_t *>(sm + kOffBar);
   const unsigned rank = (NSPLIT > 1u) ? (blockIdx.x % NSPLIT) : 0u;
   const unsigned pair = blockIdx.x / NSPLIT;
@@ -768,15 +775,17 @@ __global__ void __launch_bounds__(kThreads, 1) l1_sweep_kernel(const __grid_cons
         else
           __nanosleep(64);
       }
-      agree[0] = ok;
-      if (NSPLIT > 1u)
-        cg::this_cluster().map_shared_rank(agree, rank ^ 1u)[1] = ok;
+      for (unsigned q = 0u; q < NSPLIT; ++q)
+        cg::this_cluster().map_shared_rank(agree, q)[rank] = ok;
     }
     if (NSPLIT > 1u)
       cg::this_cluster().sync();
     else
       __syncthreads();
-    if (!agree[0] || (NSPLIT > 1u && !agree[1]))
+    unsigned all = 1u;
+    for (unsigned q = 0u; q < NSPLIT; ++q)
+      all &= agree[q];
+    if (!all)
       break; // the same decision in every CTA of the cluster
     asm volatile("fence.proxy.async;" ::: "memory"); // the copies below read what other SMs wrote
     pair_step<SORT, ACCV, NSPLIT>(P, step, pair, rank, sm);
@@ -932,6 +941,19 @@ __global__ void initV_batch_kernel(const BatchMat *const M, const unsigned nmat)
   }
 }
 
+// uniform values in (-1, 1) from a counter hash (splitmix64), for the
+// autotuner's timed runs
+__global__ void fill_random_kernel(double *const a, const size_t n, const unsigned long long seed)
+{
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    unsigned long long z = seed + 0x9e3779b97f4a7c15ull * (i + 1u);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    a[i] = (double)(long long)(z >> 11) * 0x1.0p-52 - 1.0;
+  }
+}
+
 __global__ void rsqrt_test_kernel(const double *const in, double *const out, const unsigned n)
 {
   const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1003,7 +1025,9 @@ cudaError_t l1_configure()
   cudaError_t e;
   if ((e = set_smem<false, false, 1u>(b)) || (e = set_smem<false, true, 1u>(b)) || (e = set_smem<true, false, 1u>(b)) ||
       (e = set_smem<true, true, 1u>(b)) || (e = set_smem<false, false, 2u>(b)) || (e = set_smem<false, true, 2u>(b)) ||
-      (e = set_smem<true, false, 2u>(b)) || (e = set_smem<true, true, 2u>(b)))
+      (e = set_smem<true, false, 2u>(b)) || (e = set_smem<true, true, 2u>(b)) ||
+      (e = set_smem<false, false, 4u>(b)) || (e = set_smem<false, true, 4u>(b)) ||
+      (e = set_smem<true, false, 4u>(b)) || (e = set_smem<true, true, 4u>(b)))
     return e;
   return cudaSuccess;
 }
@@ -1119,6 +1143,11 @@ template <bool S, bool A, unsigned N> static cudaError_t sweep_launch(const Step
 
 bool sweep_kernel_fits(const bool sort, const bool accv, const StepParams &p)
 {
+  if (p.split == 4u) {
+    if (sort)
+      return accv ? sweep_fits<true, true, 4u>(p) : sweep_fits<true, false, 4u>(p);
+    return accv ? sweep_fits<false, true, 4u>(p) : sweep_fits<false, false, 4u>(p);
+  }
   if (p.split == 2u) {
     if (sort)
       return accv ? sweep_fits<true, true, 2u>(p) : sweep_fits<true, false, 2u>(p);
@@ -1131,6 +1160,11 @@ bool sweep_kernel_fits(const bool sort, const bool accv, const StepParams &p)
 
 cudaError_t launch_l1_sweep(const bool sort, const bool accv, const StepParams &p, cudaStream_t s)
 {
+  if (p.split == 4u) {
+    if (sort)
+      return accv ? sweep_launch<true, true, 4u>(p, s) : sweep_launch<true, false, 4u>(p, s);
+    return accv ? sweep_launch<false, true, 4u>(p, s) : sweep_launch<false, false, 4u>(p, s);
+  }
   if (p.split == 2u) {
     if (sort)
       return accv ? sweep_launch<true, true, 2u>(p, s) : sweep_launch<true, false, 2u>(p, s);
@@ -1146,12 +1180,17 @@ unsigned l1_split(const unsigned pairs)
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess)
     (void)cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return (2u * pairs <= (unsigned)sms) ? 2u : 1u;
+  return (4u * pairs <= (unsigned)sms) ? 4u : (2u * pairs <= (unsigned)sms) ? 2u : 1u;
 }
 
 cudaError_t launch_l1_step(const bool sort, const bool accv, const StepParams &p, cudaStream_t s)
 {
   const unsigned n = p.split;
+  if (n == 4u) {
+    if (sort)
+      return accv ? launch<true, true, 4u>(p, s) : launch<true, false, 4u>(p, s);
+    return accv ? launch<false, true, 4u>(p, s) : launch<false, false, 4u>(p, s);
+  }
   if (n == 2u) {
     if (sort)
       return accv ? launch<true, true, 2u>(p, s) : launch<true, false, 2u>(p, s);
@@ -1177,6 +1216,12 @@ cudaError_t launch_initV(double *V, unsigned ncol, unsigned ldV, cudaStream_t s)
   if (blocks > 4096u)
     blocks = 4096u;
   initV_kernel<<<blocks, 256u, 0, s>>>(V, ncol, ldV);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_random(double *a, size_t n, unsigned long long seed, cudaStream_t s)
+{
+  fill_random_kernel<<<1024u, 256u, 0, s>>>(a, n, seed);
   return cudaGetLastError();
 }
 

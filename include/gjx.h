@@ -94,12 +94,30 @@ int gjx_hypJacL2_batched(unsigned routine, unsigned nmat, const unsigned *nrow, 
                          const unsigned *lddV, double *const *dD, void *stream, unsigned *sweeps,
                          unsigned long long *glb_s, unsigned long long *glb_b, int *info);
 
-/* How a sweep is launched: 1 (default) one launch per sweep, in which the
- * block pairs of consecutive outer steps start as soon as their two blocks
- * are written (used when all clusters of a step fit on the GPU at once,
- * else per step); 0 one launch per outer step, as the reference.  The
- * results are the same bits either way. */
+/* How a sweep is launched: -1 (default) the tuned choice (gjx_autotune), else
+ * per step; 0 one launch per outer step, as the reference; 1 one cooperative
+ * launch per sweep, in which the block pairs of
+ * consecutive outer steps start as soon as their two blocks are written
+ * (used when all clusters of a step fit on the GPU at once, else per step;
+ * measured no faster on a B200, kept for the autotuner).  The results are
+ * the same bits either way. */
 void gjx_set_sweep_mode(int mode);
+
+/* CTAs per block pair (a thread-block cluster): 1, 2 or 4, or 0 (default)
+ * for the automatic choice.  The results are the same bits for any value. */
+void gjx_set_split(unsigned n);
+
+/*
+ * Autotuner: time every launch configuration of this shape -- 1, 2 or 4
+ * CTAs per block pair (where the pairs fit), one launch per outer step or
+ * per sweep -- on a seeded random nrow x ncol matrix in scratch device
+ * memory, `sweeps` outer sweeps each (0: 1), and use the fastest in later
+ * calls with the same (routine, nrow, ncol, nplus) unless gjx_set_split /
+ * gjx_set_sweep_mode fix them.  out[2] = {CTAs per pair, sweep mode}.  The
+ * loaded strategy tables must match ncol.  0 or an error code.
+ */
+int gjx_autotune(unsigned routine, unsigned nrow, unsigned ncol, unsigned nplus, unsigned sweeps, unsigned *out);
+void gjx_autotune_clear(void);
 
 /* Make dev the calling thread's current device; returns its compute
  * capability as 10 * major + minor (100 for a B200), or -1.  Stands in for

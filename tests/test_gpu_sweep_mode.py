@@ -33,3 +33,26 @@ def test_one_launch_per_sweep_equals_per_step(built, m, n, p, alg, gen):
         assert np.array_equal(x.view(np.uint64), y.view(np.uint64))
     # per step: one launch per outer step; per sweep: fewer launches (one per sweep when it fits)
     assert pb["launches"] <= pa["launches"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("m,n,p,alg", [(256, 256, 256, 9), (1024, 512, 200, 11), (2048, 1024, 512, 11),
+                                       (512, 256, 0, 3)])
+def test_cluster_sizes_give_the_same_bits(built, m, n, p, alg):
+    """1, 2 or 4 CTAs per block pair, one launch per sweep or per step."""
+    import gpujachx_b200 as g
+    G = synth.make("graded", m, n, 78)
+    g.init_strats(None, "cycwor", 32, "cycwor", n // 16)
+    runs = []
+    for split in (1, 2, 4):
+        for mode in (0, 1):
+            g.lib().gjx_set_split(split)
+            g.lib().gjx_set_sweep_mode(mode)
+            runs.append(g.hypJacL2(alg, G, p))
+    g.lib().gjx_set_split(0)
+    g.lib().gjx_set_sweep_mode(1)
+    a = runs[0]
+    for b in runs[1:]:
+        assert (a.sweeps, a.rot_s, a.rot_b) == (b.sweeps, b.rot_s, b.rot_b)
+        for x, y in ((a.U, b.U), (a.D, b.D)) + (((a.V, b.V),) if alg & 2 else ()):
+            assert np.array_equal(x.view(np.uint64), y.view(np.uint64))
