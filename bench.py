@@ -425,7 +425,9 @@ def main_batch(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
-    cfg = WORKLOADS["c5"]
+    cfg = dict(WORKLOADS["c5"])
+    if args.count:
+        cfg["count"] = args.count
     sizes = batch_sizes(cfg["count"], cfg["seed"])
     if args.shard and world > 1:
         # strong scaling: one batch, split by the size-balanced partition
@@ -567,6 +569,7 @@ def main():
     ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS), help="workload (default: the headline c2)")
     ap.add_argument("--accuracy", action="store_true", help="add pp80 figures of the last decomposition")
     ap.add_argument("--shard", action="store_true", help="c5 over N ranks: split one batch instead of N batches")
+    ap.add_argument("--count", type=int, default=0, help="c5: matrices in the batch (default 4096; profiling runs)")
     args = ap.parse_args()
     _use(args.config)
     if args.impl == "reference":

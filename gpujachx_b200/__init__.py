@@ -36,7 +36,7 @@ EXPORTS = ("hypJacL2", "init_strats", "gjx_init_strats", "gjx_strat_info", "gjx_
            "gjx_version", "gjx_rsqrt_rn_dev", "gjx_profile", "gjx_profile_read", "gjx_hypJacL2_noalloc",
            "gjx_validate_pairs", "gjx_validate_strats", "gjx_configure_device", "gjx_h5_read", "gjx_h5_write",
            "gjx_hypJacL2_batched", "gjx_set_sweep_mode", "gjx_set_split", "gjx_autotune",
-           "gjx_autotune_clear")
+           "gjx_autotune_clear", "gjx_wait_selftest")
 
 
 class GjxError(RuntimeError):
@@ -99,6 +99,9 @@ def lib() -> ctypes.CDLL:
     L.gjx_hypJacL2_batched.restype = i
     L.gjx_autotune.argtypes = [u, u, u, u, u, pu]
     L.gjx_autotune.restype = i
+    L.gjx_wait_selftest.argtypes = [ctypes.c_longlong, u, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_longlong)]
+    L.gjx_wait_selftest.restype = i
     L.gjx_autotune_clear.argtypes = []
     L.gjx_autotune_clear.restype = None
     L.gjx_set_split.argtypes = [u]

@@ -1167,4 +1167,34 @@ void gjx_autotune_clear(void)
   g_tuned.clear();
 }
 
+int gjx_wait_selftest(const long long limit_cycles, const unsigned ctas, int *const timed_out,
+                      long long *const max_cycles)
+{
+  if (!ctas || ctas > 1024u || limit_cycles <= 0 || limit_cycles > (1ll << 32) || !timed_out || !max_cycles) {
+    g_err = "gjx_wait_selftest: bad arguments";
+    return -1;
+  }
+  int *d_to = nullptr;
+  long long *d_cy = nullptr;
+  GJX_CUDA(cudaMalloc(&d_to, sizeof(int)), "cudaMalloc(selftest)");
+  struct Free {
+    void *a, *b;
+    ~Free()
+    {
+      (void)cudaFree(a);
+      (void)cudaFree(b);
+    }
+  } fr{d_to, nullptr};
+  GJX_CUDA(cudaMalloc(&d_cy, ctas * sizeof(long long)), "cudaMalloc(selftest)");
+  fr.b = d_cy;
+  GJX_CUDA(cudaMemset(d_to, 0, sizeof(int)), "cudaMemset(selftest)");
+  GJX_CUDA(gjx::launch_wait_selftest(limit_cycles, d_to, d_cy, ctas, nullptr), "wait selftest");
+  GJX_CUDA(cudaDeviceSynchronize(), "wait selftest");
+  std::vector<long long> cy(ctas);
+  GJX_CUDA(cudaMemcpy(timed_out, d_to, sizeof(int), cudaMemcpyDeviceToHost), "read selftest");
+  GJX_CUDA(cudaMemcpy(cy.data(), d_cy, ctas * sizeof(long long), cudaMemcpyDeviceToHost), "read selftest");
+  *max_cycles = *std::max_element(cy.begin(), cy.end());
+  return 0;
+}
+
 } // extern "C"

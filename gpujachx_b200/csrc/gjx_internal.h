@@ -69,6 +69,7 @@ struct BatchSweep {
 
 cudaError_t batch_configure();
 cudaError_t launch_fill_random(double *a, size_t n, unsigned long long seed, cudaStream_t s);
+cudaError_t launch_wait_selftest(long long limit, int *timed_out, long long *cycles, unsigned ctas, cudaStream_t s);
 // one launch for a whole sweep (all outer steps), when every cluster of the
 // step fits on the GPU at once; false when it does not (launch per step)
 bool sweep_kernel_fits(bool sort, bool accv, const StepParams &p);

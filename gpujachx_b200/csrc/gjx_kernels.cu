@@ -941,6 +941,28 @@ __global__ void initV_batch_kernel(const BatchMat *const M, const unsigned nmat)
   }
 }
 
+// The failure path of the bounded waits, exercised on purpose: each CTA
+// waits on an mbarrier that expects one arrival nobody makes, with the given
+// cycle limit, records whether the wait gave up and in how many cycles, and
+// invalidates the barrier.  Nothing faults or hangs; the context stays usable.
+__global__ void wait_selftest_kernel(const long long limit, int *const timed_out, long long *const cycles)
+{
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0u) {
+    mbar_init(&bar, 1u);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0u) {
+    const long long t0 = clock64();
+    const bool ok = mbar_wait_bounded(&bar, 0u, limit);
+    cycles[blockIdx.x] = clock64() - t0;
+    if (!ok)
+      atomicAdd(timed_out, 1);
+    mbar_inval(&bar);
+  }
+}
+
 // uniform values in (-1, 1) from a counter hash (splitmix64), for the
 // autotuner's timed runs
 __global__ void fill_random_kernel(double *const a, const size_t n, const unsigned long long seed)
@@ -1216,6 +1238,12 @@ cudaError_t launch_initV(double *V, unsigned ncol, unsigned ldV, cudaStream_t s)
   if (blocks > 4096u)
     blocks = 4096u;
   initV_kernel<<<blocks, 256u, 0, s>>>(V, ncol, ldV);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wait_selftest(long long limit, int *timed_out, long long *cycles, unsigned ctas, cudaStream_t s)
+{
+  wait_selftest_kernel<<<ctas, 32u, 0, s>>>(limit, timed_out, cycles);
   return cudaGetLastError();
 }
 

@@ -119,6 +119,14 @@ void gjx_set_split(unsigned n);
 int gjx_autotune(unsigned routine, unsigned nrow, unsigned ncol, unsigned nplus, unsigned sweeps, unsigned *out);
 void gjx_autotune_clear(void);
 
+/* Failure-path self test of the bounded waits every kernel here uses (an
+ * mbarrier or flag that never completes makes the kernel give up after a
+ * cycle limit and report, instead of hanging): ctas CTAs each wait on an
+ * mbarrier that nobody arrives at, limit_cycles at most.  *timed_out = CTAs
+ * that gave up (all of them), *max_cycles = the longest wait.  The context
+ * stays usable.  0 or an error code. */
+int gjx_wait_selftest(long long limit_cycles, unsigned ctas, int *timed_out, long long *max_cycles);
+
 /* Make dev the calling thread's current device; returns its compute
  * capability as 10 * major + minor (100 for a B200), or -1.  Stands in for
  * configureGPU (share/cuda_helper.cu:5-54) minus its process-wide device
