@@ -65,7 +65,8 @@ __device__ __noinline__ long long rsqrt_fix_exact(long long Y, const unsigned lo
   return Y;
 }
 
-__device__ __forceinline__ double rsqrt_rn(const double a)
+// the whole method, every input class; the slow path of rsqrt_rn below
+__device__ __noinline__ double rsqrt_rn_full(const double a)
 {
   unsigned long long bits = (unsigned long long)__double_as_longlong(a);
   if ((bits >> 63) || ((bits >> 52) == 0x7FFu) || !(bits << 1)) { // negative, inf, nan, zero
@@ -103,6 +104,43 @@ __device__ __forceinline__ double rsqrt_rn(const double a)
     Yd = (double)rsqrt_fix_exact(Y, (unsigned long long)(f * pow2(52)));
   }
   return Yd * pow2(-53 - kk); // exact scaling into the normal range
+}
+
+// Fast path: the estimate from the hardware approximation (relative error
+// about 2^-20, measured) refined by one second-order Newton step to about
+// an ulp, then the same rounding decision as rsqrt_rn_full (after Markstein).
+// Whatever that decision cannot settle -- signs, zeros, subnormals, inf, NaN,
+// powers of 4 (Y = 2^53) and the rare ambiguous roundings -- goes to
+// rsqrt_rn_full in one branch at the end (the fast path's values for those
+// inputs are discarded), so the result is the correctly rounded 1/sqrt(a)
+// either way.
+__device__ __forceinline__ double rsqrt_rn(const double a)
+{
+  const unsigned long long bits = (unsigned long long)__double_as_longlong(a);
+  const unsigned long long ef = bits >> 52; // sign and exponent field
+  double y0;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(a));
+  const double h0 = a * y0;
+  const double r0 = __fma_rn(-h0, y0, 1.0);
+  const double ya = __fma_rn(y0 * r0, __fma_rn(0.375, r0, 0.5), y0); // y0 (1 + r0/2 + 3 r0^2/8)
+  const int eu = (int)ef - 1023;
+  const int k2 = eu & ~1;
+  const double f = __longlong_as_double((long long)((bits & 0xFFFFFFFFFFFFFull) | ((unsigned long long)(1023 + (eu - k2)) << 52)));
+  const int kk = k2 / 2;
+  const double y = ya * pow2(kk);
+  const double yh = y * y;
+  const double yl = __fma_rn(y, y, -yh);
+  const double e = __fma_rn(-f, yl, __fma_rn(-f, yh, 1.0));
+  // (y (e/2)) 2^53 of rsqrt_rn_full, the same bits: scalings by powers of 2 are exact
+  const double d = (y * e) * pow2(52);
+  // rint(d) for |d| < 2^51 (round to nearest even by the addition)
+  const double dr = (d + 0x1.8p52) - 0x1.8p52;
+  const double Yd = __fma_rn(y, pow2(53), dr);
+  const double res = Yd * pow2(-53 - kk);
+  if ((ef - 1ull > 2045ull) || !(fabs(d) < 0x1.0p50) || fabs(d - dr) > 0.5 - 0x1.0p-40 || Yd >= pow2(53) ||
+      Yd < pow2(52))
+    return rsqrt_rn_full(a);
+  return res;
 }
 
 // ---------------------------------------------------------------------------

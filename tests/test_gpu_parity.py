@@ -111,6 +111,31 @@ def test_rsqrt_device_equals_oracle(built, oracle):
     assert v[0] == np.inf and v[1] == -np.inf and np.isnan(v[2]) and v[3] == 0.0
 
 
+def test_rsqrt_device_bit_patterns(built, oracle):
+    """400 K inputs from raw bit patterns: every exponent of the normal range
+    with random mantissas, the powers of 2 and 4 with their neighbours (the
+    powers of 4 are the fast path's hand-off case), random subnormals; all
+    correctly rounded, equal to the oracle's."""
+    import torch
+    import gpujachx_b200 as g
+    rng = np.random.default_rng(10)
+    expo = rng.integers(1, 2047, 300000, dtype=np.uint64)
+    mant = rng.integers(0, 2 ** 52, 300000, dtype=np.uint64)
+    normal = ((expo << np.uint64(52)) | mant).view(np.float64)
+    p2 = np.ldexp(1.0, np.arange(-1022, 1024))
+    near = np.concatenate([np.nextafter(p2, 0), p2, np.nextafter(p2, np.inf)])
+    sub = (rng.integers(1, 2 ** 52, 50000, dtype=np.uint64)).view(np.float64)
+    xs = np.concatenate([normal, near, sub])
+    xs = xs[np.isfinite(xs) & (xs > 0)]
+    din = torch.tensor(xs, dtype=torch.float64, device="cuda")
+    dout = torch.empty_like(din)
+    assert g.lib().gjx_rsqrt_rn_dev(din.data_ptr(), dout.data_ptr(), len(xs)) == 0
+    got = dout.cpu().numpy()
+    want = np.array([oracle.rsqrt_rn(float(x)) for x in xs])
+    bad = np.nonzero(got.view(np.uint64) != want.view(np.uint64))[0]
+    assert bad.size == 0, (xs[bad[:5]], got[bad[:5]], want[bad[:5]])
+
+
 def test_second_call_reuses_cache(built):
     import gpujachx_b200 as g
     c = case("cache", 256, 128, 128, 9, seed=301)
