@@ -109,11 +109,11 @@ __device__ __noinline__ double rsqrt_rn_full(const double a)
 // Fast path: the estimate from the hardware approximation (relative error
 // about 2^-20, measured) refined by one second-order Newton step to about
 // an ulp, then the same rounding decision as rsqrt_rn_full (after Markstein).
-// Whatever that decision cannot settle -- signs, zeros, subnormals, inf, NaN,
-// powers of 4 (Y = 2^53) and the rare ambiguous roundings -- goes to
-// rsqrt_rn_full in one branch at the end (the fast path's values for those
-// inputs are discarded), so the result is the correctly rounded 1/sqrt(a)
-// either way.
+// Powers of 4 (f = 1) give 2^-kk exactly.  Whatever the decision cannot
+// settle -- signs, zeros, subnormals, inf, NaN and the rare ambiguous
+// roundings -- goes to rsqrt_rn_full in one branch at the end (the fast
+// path's values for those inputs are discarded), so the result is the
+// correctly rounded 1/sqrt(a) either way.
 __device__ __forceinline__ double rsqrt_rn(const double a)
 {
   const unsigned long long bits = (unsigned long long)__double_as_longlong(a);
@@ -136,9 +136,11 @@ __device__ __forceinline__ double rsqrt_rn(const double a)
   // rint(d) for |d| < 2^51 (round to nearest even by the addition)
   const double dr = (d + 0x1.8p52) - 0x1.8p52;
   const double Yd = __fma_rn(y, pow2(53), dr);
-  const double res = Yd * pow2(-53 - kk);
-  if ((ef - 1ull > 2045ull) || !(fabs(d) < 0x1.0p50) || fabs(d - dr) > 0.5 - 0x1.0p-40 || Yd >= pow2(53) ||
-      Yd < pow2(52))
+  // a power of 4 (f = 1, e.g. 1 + t^2 = 1 for a tiny rotation angle): 2^-kk exactly
+  const bool p4 = (f == 1.0);
+  const double res = p4 ? pow2(-kk) : Yd * pow2(-53 - kk);
+  if ((ef - 1ull > 2045ull) ||
+      (!p4 && (!(fabs(d) < 0x1.0p50) || fabs(d - dr) > 0.5 - 0x1.0p-40 || Yd >= pow2(53) || Yd < pow2(52))))
     return rsqrt_rn_full(a);
   return res;
 }
