@@ -486,6 +486,7 @@ def main_batch(args):
         value = args.steps * cfg["count"] / (total_ms / 1000.0)
     assert all(i == 0 for i in res.info)
     flops, nbytes = batch_flops_bytes(sizes, res.sweeps)
+    pair_steps = sum(int(sw) * (int(n) // 16 - 1) * (int(n) // 32) for n, sw in zip(sizes, res.sweeps))
     t_s = statistics.median(times) / 1000.0
     hbm, peak_kind = _peaks()
     roof = {"bound": "hbm", "achieved": nbytes / t_s / 1e9, "peak": hbm, "unit": "GB/s",
@@ -524,7 +525,10 @@ def main_batch(args):
                        "parallelism": ("one batch partitioned over ranks (size-balanced)" if (args.shard and world > 1)
                                        else "independent batches per rank" if world > 1 else "single GPU"),
                        "l2": "flushed between steps (256 MiB write, outside the timed events); inputs 3.4 GB > L2"},
-            "sweeps_max": max(res.sweeps), "sweeps_mean": float(np.mean(res.sweeps)), "e2e": e2e, "roofline": roof,
+            "sweeps_max": max(res.sweeps), "sweeps_mean": float(np.mean(res.sweeps)),
+            "block_pair_steps": pair_steps,
+            "us_per_block_pair_step_per_sm": statistics.median(times) * 1000.0 * 148 / max(1, pair_steps),
+            "e2e": e2e, "roofline": roof,
             "clocks": clk, "gpu_launches": prof["launches"] // max(1, args.steps), "step_ms": times}
     if rank == 0 and world == 1 and not args.no_cpu:
         line["plain_loop"] = plain_loop_sample(Gs, Vs, Ds, G0, offs, sizes, nplus)
