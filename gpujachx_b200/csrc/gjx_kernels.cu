@@ -6,26 +6,26 @@
 //
 //   1. Gram matrix of the M x 32 column pair [G_i G_j], lower triangle only
 //      (the Cholesky never reads the upper one).  Each CTA streams the whole
-//      pair through shared memory in 64-row tiles (16-byte cp.async into a
-//      bank-skewed layout with the wrap rows repeated, mbarrier completion,
-//      3 stages of 2 tiles) and computes its share of the 528 entries; every
+//      pair through shared memory in 64-row tiles (TMA tensor copies into a
+//      bank-skewed, zero-padded layout, mbarrier completion, 3 stages of 2
+//      tiles) and computes its share of the 528 entries; every
 //      entry is one FMA chain in the reference's row order
 //      (share/device_code_common_Cholesky.hpp:4-56).  A lane holds the 4
 //      chains (x0..x0+3, y) of one column y: the operands of column x0+u are
 //      shared by the warp, column y slides through a 4-row window, and all
 //      operands come as 16-byte row pairs.  The shares are exchanged through
 //      distributed shared memory, then one cluster barrier.
-//   2. 32x32 Cholesky by the CTA, pivots in warp 0, trailing updates over
-//      all warps (share/device_code_common_Cholesky.hpp:58-158).
-//   3. Inner Jacobi sweep(s) on R, three phases per inner step: the 48 dot
-//      products of the 16 pairs into shared memory, one lane per pair sums
-//      them in the reference's butterfly order and computes its rotation,
-//      then the warps apply the rotations to R and V_loc; trigonometric or
-//      hyperbolic rotations, optional KISS sorting
-//      (share/device_code_nosort.hpp, share/device_code_cdsort.hpp,
-//      share/device_code_cdsort_KISS.hpp).  Steps 2 and 3 are deterministic,
-//      so every CTA of the cluster computes them itself and holds the same
-//      V_loc bit for bit.
+//   2. 32x32 Cholesky by the CTA with a one-column look-ahead: warp 0 updates
+//      and pivots the next column while warps 1-7 update the rest
+//      (share/device_code_common_Cholesky.hpp:58-158).
+//   3. Inner Jacobi sweep(s) on R: per inner step each warp sums the dot
+//      products of its two pairs by register butterflies in the reference's
+//      order, half-warps compute the two rotations (branch-free; trigonometric
+//      or hyperbolic, optional KISS sorting) and every lane applies both to its
+//      row of R and V_loc; one barrier per step (share/device_code_nosort.hpp,
+//      share/device_code_cdsort.hpp, share/device_code_cdsort_KISS.hpp).
+//      Steps 2 and 3 are deterministic, so every CTA of the cluster computes
+//      them itself and holds the same V_loc bit for bit.
 //   4. [G_i G_j] <- [G_i G_j] V_loc (and V likewise): 256-row stages brought
 //      in by TMA tensor copies, the stages dealt out to the CTAs of the
 //      cluster (the first one in flight during steps 2 and 3); each output
@@ -250,9 +250,10 @@ __device__ __forceinline__ void chol32_cta(double *const R, const unsigned tid)
 //   the six dot products (Dp, Dq, Apq of both pairs) by register butterflies
 //   in the reference's order (share/device_code_common_Kepler.hpp:26-74:
 //   lane i adds lane i^16, ^8, ^4, ^2, ^1; IEEE addition commutes, so every
-//   lane ends with lane 0's bits); lanes 0-15 compute pair w's rotation,
-//   lanes 16-31 pair w+8's; the halves trade them with one shuffle; each lane
-//   applies both to its row of R and V_loc.  One barrier per step.
+//   lane ends with lane 0's bits); lanes 0-15 compute pair w's rotation
+//   (branch-free), lanes 16-31 pair w+8's; the halves trade them with one
+//   shuffle; each lane applies both to its row of R and V_loc from the values
+//   it loaded at the start of the step.  One barrier per step.
 // Every operation is the reference's (share/device_code_nosort.hpp:4-222,
 // share/device_code_cdsort.hpp:25-167, share/device_code_cdsort_KISS.hpp).
 // ---------------------------------------------------------------------------
@@ -278,74 +279,55 @@ __device__ __forceinline__ Rot inner_rot(const double Dp, const double Dq, const
                                          const unsigned q, const int definite, const unsigned npos, unsigned &ts_out,
                                          unsigned &tb_out)
 {
+  // branch-free: the two half-warps handle different pairs, so every choice
+  // below is a select of values computed by both (no divergent paths)
   Rot r;
-  r.c = 1.0;
-  r.t = 0.0;
-  r.t_ = 0.0;
-  r.mode = 0;
-  r.scale = 0;
-  r.swap = 0;
   const double Dp_ = __dsqrt_rn(Dp), Dq_ = __dsqrt_rn(Dq), Apq_ = fabs(Apq), Dpq_ = Dp_ * Dq_;
   const int ts = !(Apq_ < (Dpq_ * kMyTol));
-  int tb = 0;
+  int tb;
   if (!SORT) {
     // the rotation is computed whether or not it is applied (no side
     // effects), so that its latency overlaps the relative test
     const bool trig = definite || ((p < npos) && (q < npos)) || ((p >= npos) && (q >= npos));
     double c, t;
     const int b = rot_either(trig, Apq, Dp, Dq, c, t);
-    if (ts) {
-      r.c = c;
-      r.t = t;
-      r.t_ = trig ? -t : t;
-      tb = b;
-      r.mode = 1;
-      r.scale = tb;
-    }
+    r.c = ts ? c : 1.0;
+    r.t = ts ? t : 0.0;
+    r.t_ = ts ? (trig ? -t : t) : 0.0;
+    tb = ts ? b : 0;
+    r.mode = ts;
+    r.scale = tb;
+    r.swap = 0;
   }
   else {
-    int def;
-    if (definite)
-      def = definite;
-    else if ((p < npos) && (q < npos))
-      def = +1;
-    else if ((p >= npos) && (q >= npos))
-      def = -1;
-    else
-      def = 0;
+    const int def = definite ? definite : ((p < npos) && (q < npos)) ? +1 : ((p >= npos) && (q >= npos)) ? -1 : 0;
     double c, t;
     const int b = rot_either(def != 0, Apq, Dp, Dq, c, t);
-    if (ts) {
-      double Dp2 = Dp, Dq2 = Dq;
-      r.c = c;
-      r.t = t;
-      tb = b;
-      if (def) {
-        r.t_ = -t;
-        Dp2 = __fma_rn(t, Apq, Dp);
-        Dq2 = __fma_rn(r.t_, Apq, Dq);
-      }
-      else
-        r.t_ = t;
-      r.mode = 1;
-      r.scale = tb;
-      r.swap = !((!def) || ((def > 0) && (Dp2 >= Dq2)) || ((def < 0) && (Dp2 <= Dq2)));
-    }
-    else if (((def > 0) && (Dp < Dq)) || ((def < 0) && (Dq < Dp)))
-      r.mode = 2;
+    const double t_ = def ? -t : t;
+    const double Dp2 = __fma_rn(t, Apq, Dp), Dq2 = __fma_rn(t_, Apq, Dq); // used when ts and def
+    const int swp = !((!def) || ((def > 0) && (Dp2 >= Dq2)) || ((def < 0) && (Dp2 <= Dq2)));
+    const int order = ((def > 0) && (Dp < Dq)) || ((def < 0) && (Dq < Dp));
+    r.c = ts ? c : 1.0;
+    r.t = ts ? t : 0.0;
+    r.t_ = ts ? t_ : 0.0;
+    tb = ts ? b : 0;
+    r.mode = ts ? 1 : (order ? 2 : 0);
+    r.scale = tb;
+    r.swap = ts ? swp : 0;
   }
   ts_out = (unsigned)ts;
   tb_out = (unsigned)tb;
   return r;
 }
 
+// apply rotation r to row x of columns p, q of R (values Gp, Gq, already
+// loaded) and of V_loc (Vp, Vq); mode 0 leaves them, 2 swaps the columns
 __device__ __forceinline__ void inner_apply(double *const R, double *const Vl, const unsigned p, const unsigned q,
-                                            const Rot &r, const unsigned x)
+                                            const Rot &r, const unsigned x, const double Gp, const double Gq,
+                                            const double Vp, const double Vq)
 {
   if (r.mode == 0)
     return;
-  const double Gp = E32(R, x, p), Gq = E32(R, x, q);
-  const double Vp = E32(Vl, x, p), Vq = E32(Vl, x, q);
   if (r.mode == 2) {
     E32(R, x, p) = Gq;
     E32(R, x, q) = Gp;
@@ -383,6 +365,8 @@ __device__ __forceinline__ void inner_sweeps(double *const R, double *const Vl, 
       const uint8_t *const st = s0 + step * 32u;
       const unsigned pa = st[2u * w], qa = st[2u * w + 1u], pb = st[2u * w + 16u], qb = st[2u * w + 17u];
       const double Gpa = E32(R, x, pa), Gqa = E32(R, x, qa), Gpb = E32(R, x, pb), Gqb = E32(R, x, qb);
+      // V_loc of the same rows, loaded now so that the application waits for no load
+      const double Vpa = E32(Vl, x, pa), Vqa = E32(Vl, x, qa), Vpb = E32(Vl, x, pb), Vqb = E32(Vl, x, qb);
       double v[6] = {__fma_rn(Gpa, Gpa, 0.0), __fma_rn(Gqa, Gqa, 0.0), __fma_rn(Gpa, Gqa, 0.0),
                      __fma_rn(Gpb, Gpb, 0.0), __fma_rn(Gqb, Gqb, 0.0), __fma_rn(Gpb, Gqb, 0.0)};
 #pragma unroll
@@ -395,9 +379,9 @@ __device__ __forceinline__ void inner_sweeps(double *const R, double *const Vl, 
         for (unsigned i = 0u; i < 6u; ++i)
           v[i] = v[i] + o[i];
       }
+      const double Dp = hb ? v[3] : v[0], Dq = hb ? v[4] : v[1], Apq = hb ? v[5] : v[2];
       unsigned a_s, a_b;
-      const Rot r = inner_rot<SORT>(hb ? v[3] : v[0], hb ? v[4] : v[1], hb ? v[5] : v[2], hb ? pb : pa,
-                                    hb ? qb : qa, definite, npos, a_s, a_b);
+      const Rot r = inner_rot<SORT>(Dp, Dq, Apq, hb ? pb : pa, hb ? qb : qa, definite, npos, a_s, a_b);
       if (x == 0u || x == 16u) {
         ws += a_s;
         wb += a_b;
@@ -410,8 +394,8 @@ __device__ __forceinline__ void inner_sweeps(double *const R, double *const Vl, 
       o.mode = fl & 3;
       o.scale = (fl >> 2) & 1;
       o.swap = (fl >> 3) & 1;
-      inner_apply(R, Vl, pa, qa, hb ? o : r, x);
-      inner_apply(R, Vl, pb, qb, hb ? r : o, x);
+      inner_apply(R, Vl, pa, qa, hb ? o : r, x, Gpa, Gqa, Vpa, Vqa);
+      inner_apply(R, Vl, pb, qb, hb ? r : o, x, Gpb, Gqb, Vpb, Vqb);
       __syncthreads();
     }
     ws = __reduce_add_sync(0xffffffffu, ws);
