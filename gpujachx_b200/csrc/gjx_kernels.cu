@@ -367,19 +367,30 @@ __device__ __forceinline__ void inner_sweeps(double *const R, double *const Vl, 
       const double Gpa = E32(R, x, pa), Gqa = E32(R, x, qa), Gpb = E32(R, x, pb), Gqb = E32(R, x, qb);
       // V_loc of the same rows, loaded now so that the application waits for no load
       const double Vpa = E32(Vl, x, pa), Vqa = E32(Vl, x, qa), Vpb = E32(Vl, x, pb), Vqb = E32(Vl, x, qb);
-      double v[6] = {__fma_rn(Gpa, Gpa, 0.0), __fma_rn(Gqa, Gqa, 0.0), __fma_rn(Gpa, Gqa, 0.0),
-                     __fma_rn(Gpb, Gpb, 0.0), __fma_rn(Gqb, Gqb, 0.0), __fma_rn(Gpb, Gqb, 0.0)};
+      // the butterfly as a reduce-scatter: at the first level (lane ^ 16) each
+      // lane keeps the products of its half's pair and receives the partner's
+      // products of the same pair; the other four levels stay within the half.
+      // Every lane adds the same operands in the same order as the full
+      // butterfly would, with half the shuffles.
+      const double va[3] = {__fma_rn(Gpa, Gpa, 0.0), __fma_rn(Gqa, Gqa, 0.0), __fma_rn(Gpa, Gqa, 0.0)};
+      const double vb[3] = {__fma_rn(Gpb, Gpb, 0.0), __fma_rn(Gqb, Gqb, 0.0), __fma_rn(Gpb, Gqb, 0.0)};
+      double v[3];
 #pragma unroll
-      for (unsigned k = 16u; k; k >>= 1u) {
-        double o[6];
+      for (unsigned i = 0u; i < 3u; ++i) {
+        const double other = __shfl_xor_sync(0xffffffffu, hb ? va[i] : vb[i], 16);
+        v[i] = (hb ? vb[i] : va[i]) + other;
+      }
 #pragma unroll
-        for (unsigned i = 0u; i < 6u; ++i)
+      for (unsigned k = 8u; k; k >>= 1u) {
+        double o[3];
+#pragma unroll
+        for (unsigned i = 0u; i < 3u; ++i)
           o[i] = __shfl_xor_sync(0xffffffffu, v[i], k);
 #pragma unroll
-        for (unsigned i = 0u; i < 6u; ++i)
+        for (unsigned i = 0u; i < 3u; ++i)
           v[i] = v[i] + o[i];
       }
-      const double Dp = hb ? v[3] : v[0], Dq = hb ? v[4] : v[1], Apq = hb ? v[5] : v[2];
+      const double Dp = v[0], Dq = v[1], Apq = v[2];
       unsigned a_s, a_b;
       const Rot r = inner_rot<SORT>(Dp, Dq, Apq, hb ? pb : pa, hb ? qb : qa, definite, npos, a_s, a_b);
       if (x == 0u || x == 16u) {
