@@ -443,6 +443,8 @@ def main_batch(args):
         G0, offs = batch_inputs(sizes, dev, cfg["seed"] + rank)
     nplus = [int(n) if b % 2 == 0 else int(n) // 2 for b, n in enumerate(sizes)]
     g.init_strats(None, "cycwor", 32, "cycwor", 4)
+    width = 1 if os.environ.get("GJX_BATCH_WIDTH") == "1" else 2  # block pairs per CTA at a time
+    g.lib().gjx_set_batch_width(width)
     dG = torch.empty_like(G0)
     dV = torch.empty_like(G0)
     dD = torch.empty(int(sizes.sum()), dtype=torch.float64, device=dev)
@@ -522,6 +524,7 @@ def main_batch(args):
             "scaling": "strong" if (args.shard and world > 1) else "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": cfg["workload"], "name": "c5", "count": nmat, "alg": ALG,
+                       "block_pairs_per_cta": width,
                        "parallelism": ("one batch partitioned over ranks (size-balanced)" if (args.shard and world > 1)
                                        else "independent batches per rank" if world > 1 else "single GPU"),
                        "l2": "flushed between steps (256 MiB write, outside the timed events); inputs 3.4 GB > L2"},

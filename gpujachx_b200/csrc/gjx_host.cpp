@@ -50,6 +50,7 @@ Strat g_strat;
 int g_verbose = 1;
 int g_sweep_mode = -1; // -1 automatic (the tuned choice, else per step), 0 per outer step, 1 one launch per sweep
 unsigned g_split = 0u;  // CTAs per block pair: 0 automatic (the tuned choice, else by the SM count), else 1, 2, 4
+unsigned g_batch_width = 2u; // block pairs a CTA of the batched form takes at a time: 1 or 2
 
 // the autotuner's choices, by (routine, nrow, ncol, nplus)
 struct TuneKey {
@@ -560,7 +561,7 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
   const gjx::BatchSweep sw{d_mats, d_ks, d_cvg, d_done, d_swp, d_gs, d_gb, d_q, d_act, nmat};
   const unsigned ctas = std::min<unsigned>((unsigned)sms, (unsigned)items.size());
   for (unsigned k = 0u; k < kLaunches && ce == cudaSuccess; ++k) {
-    ce = gjx::launch_batch_step(cdsort, full, bs, ctas, st);
+    ce = gjx::launch_batch_step(cdsort, full, g_batch_width, bs, ctas, st);
     if (ce == cudaSuccess)
       ce = cudaMemsetAsync(d_act, 0, 4u, st); // the count of the last launch is the one read
     if (ce == cudaSuccess)
@@ -1073,6 +1074,12 @@ void gjx_set_split(const unsigned n)
 {
   std::lock_guard<std::mutex> lk(g_mtx);
   g_split = (n == 1u || n == 2u || n == 4u) ? n : 0u;
+}
+
+void gjx_set_batch_width(const unsigned w)
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  g_batch_width = (w == 1u) ? 1u : 2u;
 }
 
 int gjx_autotune(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,

@@ -74,7 +74,9 @@ cudaError_t launch_wait_selftest(long long limit, int *timed_out, long long *cyc
 // step fits on the GPU at once; false when it does not (launch per step)
 bool sweep_kernel_fits(bool sort, bool accv, const StepParams &p);
 cudaError_t launch_l1_sweep(bool sort, bool accv, const StepParams &p, cudaStream_t s);
-cudaError_t launch_batch_step(bool sort, bool accv, const BatchStep &b, unsigned ctas, cudaStream_t s);
+// width 1: one block pair per CTA at a time; 2: two (pair_step2)
+cudaError_t launch_batch_step(bool sort, bool accv, unsigned width, const BatchStep &b, unsigned ctas,
+                              cudaStream_t s);
 cudaError_t launch_batch_sweep_end(const BatchSweep &w, cudaStream_t s);
 cudaError_t launch_batch_initV(const BatchMat *m, unsigned nmat, cudaStream_t s);
 cudaError_t launch_batch_initD(const BatchMat *m, unsigned nmat, const uint32_t *ok, cudaStream_t s);
@@ -88,6 +90,7 @@ cudaError_t make_gram_map(CUtensorMap *tm, const double *base, unsigned nrow, un
 enum : int { kErrWaitTimeout = 1 };
 
 size_t l1_smem_bytes();
+size_t batch2_smem_bytes();
 cudaError_t l1_configure();
 cudaError_t launch_l1_step(bool sort, bool accv, const StepParams &p, cudaStream_t s);
 // CTAs per block pair for `pairs` pairs per step on the current device

@@ -207,12 +207,22 @@ __device__ __forceinline__ void chol_pivot(double *const R, const unsigned j, co
     E32(R, j, j) = sq;
 }
 
-__device__ __forceinline__ void chol32_cta(double *const R, const unsigned tid)
+// a named barrier for the nthreads threads of a warp group (id 0 with all the
+// CTA's threads is __syncthreads)
+__device__ __forceinline__ void bar_sync(const unsigned id, const unsigned nthreads)
 {
-  const unsigned w = tid >> 5, x = tid & 31u;
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// by a group of NW warps (thread gt of the group, named barrier bar): the
+// group's warp 0 pivots, warps 1..NW-1 update the trailing columns
+template <unsigned NW>
+__device__ __forceinline__ void chol32_grp(double *const R, const unsigned gt, const unsigned bar)
+{
+  const unsigned w = gt >> 5, x = gt & 31u;
   if (w == 0u)
     chol_pivot(R, 0u, x, E32(R, x, 0u));
-  __syncthreads();
+  bar_sync(bar, NW * 32u);
 #pragma unroll 1
   for (unsigned k = 0u; k + 1u < 32u; ++k) {
     if (w == 0u) {
@@ -224,22 +234,23 @@ __device__ __forceinline__ void chol32_cta(double *const R, const unsigned tid)
     }
     else {
 #pragma unroll 1
-      for (unsigned j = k + 1u + w; j < 32u; j += kThreads / 32u - 1u)
+      for (unsigned j = k + 1u + w; j < 32u; j += NW - 1u)
         if (x >= j)
           E32(R, x, j) = __fma_rn(-E32(R, x, k), E32(R, j, k), E32(R, x, j));
     }
-    __syncthreads();
+    bar_sync(bar, NW * 32u);
   }
-  double v[4];
+  constexpr unsigned NV = 1024u / (NW * 32u);
+  double v[NV];
 #pragma unroll
-  for (unsigned i = 0u; i < 4u; ++i) { // element (x = col of R^T, y = row) = (i*256 + tid)
-    const unsigned e = i * kThreads + tid, xx = e >> 5, yy = e & 31u;
+  for (unsigned i = 0u; i < NV; ++i) { // element (x = col of R^T, y = row) = (i*NW*32 + gt)
+    const unsigned e = i * NW * 32u + gt, xx = e >> 5, yy = e & 31u;
     v[i] = (xx >= yy) ? E32(R, xx, yy) : 0.0;
   }
-  __syncthreads();
+  bar_sync(bar, NW * 32u);
 #pragma unroll
-  for (unsigned i = 0u; i < 4u; ++i) {
-    const unsigned e = i * kThreads + tid, xx = e >> 5, yy = e & 31u;
+  for (unsigned i = 0u; i < NV; ++i) {
+    const unsigned e = i * NW * 32u + gt, xx = e >> 5, yy = e & 31u;
     E32(R, yy, xx) = v[i];
   }
 }
@@ -350,64 +361,96 @@ __device__ __forceinline__ void inner_apply(double *const R, double *const Vl, c
   E32(Vl, x, dq) = vq;
 }
 
-template <bool SORT>
+// by a group of NW warps (8 or 4; lane x, warp w of the group, named barrier
+// bar): warp w takes the NC = 8 / NW couples of pairs (w + c NW, w + c NW + 8)
+// of each inner step, interleaved
+template <bool SORT, unsigned NW>
 __device__ __forceinline__ void inner_sweeps(double *const R, double *const Vl, const uint8_t *const s0,
                                              const unsigned s0steps, const unsigned nswp, const int definite,
                                              const unsigned npos, unsigned *const red, const unsigned x,
-                                             const unsigned w, unsigned &blk_s, unsigned &blk_b)
+                                             const unsigned w, const unsigned bar, unsigned &blk_s, unsigned &blk_b)
 {
+  constexpr unsigned NC = 8u / NW;
   blk_s = 0u;
   blk_b = 0u;
-  const bool hb = x >= 16u; // this half computes pair w + 8 (else pair w)
+  const bool hb = x >= 16u; // this half computes the couple's second pair (else its first)
   for (unsigned swp = 0u; swp < nswp; ++swp) {
-    unsigned ws = 0u, wb = 0u; // lanes 0 and 16: their pair's counts
+    unsigned ws = 0u, wb = 0u; // lanes 0 and 16: their pairs' counts
     for (unsigned step = 0u; step < s0steps; ++step) {
       const uint8_t *const st = s0 + step * 32u;
-      const unsigned pa = st[2u * w], qa = st[2u * w + 1u], pb = st[2u * w + 16u], qb = st[2u * w + 17u];
-      const double Gpa = E32(R, x, pa), Gqa = E32(R, x, qa), Gpb = E32(R, x, pb), Gqb = E32(R, x, qb);
-      // V_loc of the same rows, loaded now so that the application waits for no load
-      const double Vpa = E32(Vl, x, pa), Vqa = E32(Vl, x, qa), Vpb = E32(Vl, x, pb), Vqb = E32(Vl, x, qb);
-      // the butterfly as a reduce-scatter: at the first level (lane ^ 16) each
-      // lane keeps the products of its half's pair and receives the partner's
-      // products of the same pair; the other four levels stay within the half.
-      // Every lane adds the same operands in the same order as the full
-      // butterfly would, with half the shuffles.
-      const double va[3] = {__fma_rn(Gpa, Gpa, 0.0), __fma_rn(Gqa, Gqa, 0.0), __fma_rn(Gpa, Gqa, 0.0)};
-      const double vb[3] = {__fma_rn(Gpb, Gpb, 0.0), __fma_rn(Gqb, Gqb, 0.0), __fma_rn(Gpb, Gqb, 0.0)};
-      double v[3];
+      unsigned pa[NC], qa[NC], pb[NC], qb[NC];
+      double Gpa[NC], Gqa[NC], Gpb[NC], Gqb[NC], Vpa[NC], Vqa[NC], Vpb[NC], Vqb[NC], v[NC][3];
 #pragma unroll
-      for (unsigned i = 0u; i < 3u; ++i) {
-        const double other = __shfl_xor_sync(0xffffffffu, hb ? va[i] : vb[i], 16);
-        v[i] = (hb ? vb[i] : va[i]) + other;
+      for (unsigned c = 0u; c < NC; ++c) {
+        const unsigned a = w + c * NW;
+        pa[c] = st[2u * a];
+        qa[c] = st[2u * a + 1u];
+        pb[c] = st[2u * a + 16u];
+        qb[c] = st[2u * a + 17u];
+        Gpa[c] = E32(R, x, pa[c]);
+        Gqa[c] = E32(R, x, qa[c]);
+        Gpb[c] = E32(R, x, pb[c]);
+        Gqb[c] = E32(R, x, qb[c]);
+        // V_loc of the same rows, loaded now so that the application waits for no load
+        Vpa[c] = E32(Vl, x, pa[c]);
+        Vqa[c] = E32(Vl, x, qa[c]);
+        Vpb[c] = E32(Vl, x, pb[c]);
+        Vqb[c] = E32(Vl, x, qb[c]);
+        // the butterfly as a reduce-scatter: at the first level (lane ^ 16)
+        // each lane keeps the products of its half's pair and receives the
+        // partner's products of the same pair; the other four levels stay
+        // within the half.  Every lane adds the same operands in the same
+        // order as the full butterfly would, with half the shuffles.
+        const double va[3] = {__fma_rn(Gpa[c], Gpa[c], 0.0), __fma_rn(Gqa[c], Gqa[c], 0.0),
+                              __fma_rn(Gpa[c], Gqa[c], 0.0)};
+        const double vb[3] = {__fma_rn(Gpb[c], Gpb[c], 0.0), __fma_rn(Gqb[c], Gqb[c], 0.0),
+                              __fma_rn(Gpb[c], Gqb[c], 0.0)};
+#pragma unroll
+        for (unsigned i = 0u; i < 3u; ++i) {
+          const double other = __shfl_xor_sync(0xffffffffu, hb ? va[i] : vb[i], 16);
+          v[c][i] = (hb ? vb[i] : va[i]) + other;
+        }
       }
 #pragma unroll
       for (unsigned k = 8u; k; k >>= 1u) {
-        double o[3];
+        double o[NC][3];
 #pragma unroll
-        for (unsigned i = 0u; i < 3u; ++i)
-          o[i] = __shfl_xor_sync(0xffffffffu, v[i], k);
+        for (unsigned c = 0u; c < NC; ++c)
 #pragma unroll
-        for (unsigned i = 0u; i < 3u; ++i)
-          v[i] = v[i] + o[i];
+          for (unsigned i = 0u; i < 3u; ++i)
+            o[c][i] = __shfl_xor_sync(0xffffffffu, v[c][i], k);
+#pragma unroll
+        for (unsigned c = 0u; c < NC; ++c)
+#pragma unroll
+          for (unsigned i = 0u; i < 3u; ++i)
+            v[c][i] = v[c][i] + o[c][i];
       }
-      const double Dp = v[0], Dq = v[1], Apq = v[2];
-      unsigned a_s, a_b;
-      const Rot r = inner_rot<SORT>(Dp, Dq, Apq, hb ? pb : pa, hb ? qb : qa, definite, npos, a_s, a_b);
-      if (x == 0u || x == 16u) {
-        ws += a_s;
-        wb += a_b;
+      Rot r[NC];
+#pragma unroll
+      for (unsigned c = 0u; c < NC; ++c) {
+        unsigned a_s, a_b;
+        r[c] = inner_rot<SORT>(v[c][0], v[c][1], v[c][2], hb ? pb[c] : pa[c], hb ? qb[c] : qa[c], definite, npos, a_s,
+                               a_b);
+        if (x == 0u || x == 16u) {
+          ws += a_s;
+          wb += a_b;
+        }
       }
-      Rot o;
-      o.c = __shfl_xor_sync(0xffffffffu, r.c, 16);
-      o.t = __shfl_xor_sync(0xffffffffu, r.t, 16);
-      o.t_ = __shfl_xor_sync(0xffffffffu, r.t_, 16);
-      const int fl = __shfl_xor_sync(0xffffffffu, r.mode | (r.scale << 2) | (r.swap << 3), 16);
-      o.mode = fl & 3;
-      o.scale = (fl >> 2) & 1;
-      o.swap = (fl >> 3) & 1;
-      inner_apply(R, Vl, pa, qa, hb ? o : r, x, Gpa, Gqa, Vpa, Vqa);
-      inner_apply(R, Vl, pb, qb, hb ? r : o, x, Gpb, Gqb, Vpb, Vqb);
-      __syncthreads();
+#pragma unroll
+      for (unsigned c = 0u; c < NC; ++c) {
+        Rot o;
+        o.c = __shfl_xor_sync(0xffffffffu, r[c].c, 16);
+        o.t = __shfl_xor_sync(0xffffffffu, r[c].t, 16);
+        o.t_ = __shfl_xor_sync(0xffffffffu, r[c].t_, 16);
+        const int fl = __shfl_xor_sync(0xffffffffu, r[c].mode | (r[c].scale << 2) | (r[c].swap << 3), 16);
+        o.mode = fl & 3;
+        o.scale = (fl >> 2) & 1;
+        o.swap = (fl >> 3) & 1;
+        const Rot m = r[c]; // a value: selecting between two lvalues would take their addresses
+        inner_apply(R, Vl, pa[c], qa[c], hb ? o : m, x, Gpa[c], Gqa[c], Vpa[c], Vqa[c]);
+        inner_apply(R, Vl, pb[c], qb[c], hb ? m : o, x, Gpb[c], Gqb[c], Vpb[c], Vqb[c]);
+      }
+      bar_sync(bar, NW * 32u);
     }
     ws = __reduce_add_sync(0xffffffffu, ws);
     wb = __reduce_add_sync(0xffffffffu, wb);
@@ -415,14 +458,119 @@ __device__ __forceinline__ void inner_sweeps(double *const R, double *const Vl, 
       red[2u * w] = ws;
       red[2u * w + 1u] = wb;
     }
-    __syncthreads();
+    bar_sync(bar, NW * 32u);
     unsigned tot_s = 0u, tot_b = 0u;
 #pragma unroll
-    for (unsigned k = 0u; k < kThreads / 32u; ++k) {
+    for (unsigned k = 0u; k < NW; ++k) {
       tot_s += red[2u * k];
       tot_b += red[2u * k + 1u];
     }
-    __syncthreads();
+    bar_sync(bar, NW * 32u);
+    if (tot_s) {
+      blk_s += tot_s;
+      blk_b += tot_b;
+    }
+    else
+      break;
+  }
+}
+
+// by a group of 4 warps (lane x, warp w of the group, named barrier bar):
+// warp w takes pairs w, w + 4, w + 8, w + 12 of each inner step, and quarter
+// k of the warp (lanes 8k .. 8k + 7) computes pair w + 4k's rotation.  The
+// twelve dot products go through a reduce-scatter: at level 16 each half
+// keeps its two pairs' products (lanes 0-15 pairs w, w + 4), at level 8 each
+// quarter its own pair's, levels 4, 2, 1 stay within the quarter -- the same
+// operands in the same order as the full butterfly, with one rotation to
+// evaluate per warp and step.  Every lane then applies the four rotations.
+template <bool SORT>
+__device__ __forceinline__ void inner_sweeps_q(double *const R, double *const Vl, const uint8_t *const s0,
+                                               const unsigned s0steps, const unsigned nswp, const int definite,
+                                               const unsigned npos, unsigned *const red, const unsigned x,
+                                               const unsigned w, const unsigned bar, unsigned &blk_s,
+                                               unsigned &blk_b)
+{
+  blk_s = 0u;
+  blk_b = 0u;
+  const bool up = x >= 16u, odd = ((x >> 3) & 1u) != 0u;
+  const unsigned mine = w + 4u * (x >> 3); // the pair this lane's quarter evaluates
+  for (unsigned swp = 0u; swp < nswp; ++swp) {
+    unsigned ws = 0u, wb = 0u; // lanes 0, 8, 16, 24: their pairs' counts
+    for (unsigned step = 0u; step < s0steps; ++step) {
+      const uint8_t *const st = s0 + step * 32u;
+      unsigned p[4], q[4];
+      double Gp[4], Gq[4], Vp[4], Vq[4], v[4][3];
+#pragma unroll
+      for (unsigned k = 0u; k < 4u; ++k) {
+        p[k] = st[2u * (w + 4u * k)];
+        q[k] = st[2u * (w + 4u * k) + 1u];
+        Gp[k] = E32(R, x, p[k]);
+        Gq[k] = E32(R, x, q[k]);
+        Vp[k] = E32(Vl, x, p[k]);
+        Vq[k] = E32(Vl, x, q[k]);
+        v[k][0] = __fma_rn(Gp[k], Gp[k], 0.0);
+        v[k][1] = __fma_rn(Gq[k], Gq[k], 0.0);
+        v[k][2] = __fma_rn(Gp[k], Gq[k], 0.0);
+      }
+      const unsigned pm = st[2u * mine], qm = st[2u * mine + 1u];
+      double h[2][3], s[3];
+#pragma unroll
+      for (unsigned j = 0u; j < 2u; ++j)
+#pragma unroll
+        for (unsigned i = 0u; i < 3u; ++i) {
+          const double other = __shfl_xor_sync(0xffffffffu, up ? v[j][i] : v[2u + j][i], 16);
+          h[j][i] = (up ? v[2u + j][i] : v[j][i]) + other;
+        }
+#pragma unroll
+      for (unsigned i = 0u; i < 3u; ++i) {
+        const double other = __shfl_xor_sync(0xffffffffu, odd ? h[0][i] : h[1][i], 8);
+        s[i] = (odd ? h[1][i] : h[0][i]) + other;
+      }
+#pragma unroll
+      for (unsigned k = 4u; k; k >>= 1u) {
+        double o[3];
+#pragma unroll
+        for (unsigned i = 0u; i < 3u; ++i)
+          o[i] = __shfl_xor_sync(0xffffffffu, s[i], k);
+#pragma unroll
+        for (unsigned i = 0u; i < 3u; ++i)
+          s[i] = s[i] + o[i];
+      }
+      unsigned a_s, a_b;
+      const Rot r = inner_rot<SORT>(s[0], s[1], s[2], pm, qm, definite, npos, a_s, a_b);
+      if (!(x & 7u)) {
+        ws += a_s;
+        wb += a_b;
+      }
+      const int fl = r.mode | (r.scale << 2) | (r.swap << 3);
+#pragma unroll
+      for (unsigned k = 0u; k < 4u; ++k) {
+        Rot o;
+        o.c = __shfl_sync(0xffffffffu, r.c, 8 * k);
+        o.t = __shfl_sync(0xffffffffu, r.t, 8 * k);
+        o.t_ = __shfl_sync(0xffffffffu, r.t_, 8 * k);
+        const int f = __shfl_sync(0xffffffffu, fl, 8 * k);
+        o.mode = f & 3;
+        o.scale = (f >> 2) & 1;
+        o.swap = (f >> 3) & 1;
+        inner_apply(R, Vl, p[k], q[k], o, x, Gp[k], Gq[k], Vp[k], Vq[k]);
+      }
+      bar_sync(bar, 128u);
+    }
+    ws = __reduce_add_sync(0xffffffffu, ws);
+    wb = __reduce_add_sync(0xffffffffu, wb);
+    if (x == 0u) {
+      red[2u * w] = ws;
+      red[2u * w + 1u] = wb;
+    }
+    bar_sync(bar, 128u);
+    unsigned tot_s = 0u, tot_b = 0u;
+#pragma unroll
+    for (unsigned k = 0u; k < 4u; ++k) {
+      tot_s += red[2u * k];
+      tot_b += red[2u * k + 1u];
+    }
+    bar_sync(bar, 128u);
     if (tot_s) {
       blk_s += tot_s;
       blk_b += tot_b;
@@ -468,6 +616,77 @@ __device__ __forceinline__ void update_stage(const double *const st, const doubl
           acc[u][v] = __fma_rn(a[u], b[v], acc[u][v]);
       }
   }
+}
+
+// stores of one stage's tile: lanes l and l^8 own the same 4 rows of column
+// groups 2h and 2h+1; they trade halves so that each store instruction fills
+// whole 32-byte sectors (rows r0..r0+1 from the even lane, r0+2..r0+3 from
+// the odd one, same column).  Rows past the end (a stage of rows < 256) are
+// not stored.
+__device__ __forceinline__ void update_store(const double (&acc)[4][8], double *const ci, double *const cj,
+                                             const size_t ld, const unsigned base, const unsigned rows,
+                                             const unsigned rg, const unsigned sub, const unsigned cg8)
+{
+  const bool live = sub * 32u < rows;
+  const unsigned r0 = base + sub * 32u + rg * 4u;
+  const bool even = !(cg8 & 1u);
+  const unsigned ce = (cg8 & ~1u) * 8u, roff = even ? 0u : 2u;
+#pragma unroll
+  for (unsigned v = 0u; v < 8u; ++v) {
+    const double s0v = even ? acc[2][v] : acc[0][v], s1v = even ? acc[3][v] : acc[1][v];
+    const double r0v = __shfl_xor_sync(0xffffffffu, s0v, 8), r1v = __shfl_xor_sync(0xffffffffu, s1v, 8);
+    if (live) {
+      const unsigned c1 = ce + v, c2 = ce + 8u + v;
+      double *const col1 = ((c1 < 16u) ? (ci + (size_t)c1 * ld) : (cj + (size_t)(c1 - 16u) * ld)) + r0 + roff;
+      double *const col2 = ((c2 < 16u) ? (ci + (size_t)c2 * ld) : (cj + (size_t)(c2 - 16u) * ld)) + r0 + roff;
+      *reinterpret_cast<double2 *>(col1) = even ? make_double2(acc[0][v], acc[1][v]) : make_double2(r0v, r1v);
+      *reinterpret_cast<double2 *>(col2) = even ? make_double2(r0v, r1v) : make_double2(acc[2][v], acc[3][v]);
+    }
+  }
+}
+
+// the signature of block pair (iBlk, jBlk): global if the matrix is definite,
+// else block-local (share/device_code_nosort_solveV.hpp:33-67)
+__device__ __forceinline__ void block_signature(const StepParams &P, const unsigned iBlk, const unsigned jBlk,
+                                                int &definite, unsigned &npos)
+{
+  const unsigned ifc0 = iBlk * kNColB, ifc1 = jBlk * kNColB, nplus = P.nplus;
+  if (P.gdefinite) {
+    definite = P.gdefinite;
+    npos = 0u;
+  }
+  else if (nplus <= ifc0) {
+    npos = 0u;
+    definite = -1;
+  }
+  else if (nplus <= ifc0 + kNColB) {
+    npos = nplus - ifc0;
+    definite = 0;
+  }
+  else if (nplus <= ifc1) {
+    npos = kNColB;
+    definite = 0;
+  }
+  else if (nplus <= ifc1 + kNColB) {
+    npos = kNColB + (nplus - ifc1);
+    definite = 0;
+  }
+  else {
+    npos = 2u * kNColB;
+    definite = +1;
+  }
+}
+
+// a block pair's rotation counts into its matrix's sweep counter: big << 32 |
+// small, or the low word alone when no rotation was big, as the reference
+__device__ __forceinline__ void add_counts(const StepParams &P, const unsigned blk_s, const unsigned blk_b)
+{
+  if (!blk_s)
+    return;
+  if (blk_b)
+    atomicAdd(P.cvg, (((unsigned long long)blk_b) << 32) | blk_s);
+  else
+    atomicAdd(reinterpret_cast<unsigned *>(P.cvg), blk_s);
 }
 
 // ---------------------------------------------------------------------------
@@ -592,48 +811,18 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
   // ---------------------------- 2. Cholesky -------------------------------
   for (unsigned i = tid; i < 1024u; i += kThreads)
     Vl[i] = ((i >> 5) == (i & 31u)) ? 1.0 : 0.0;
-  chol32_cta(R, tid);
+  chol32_grp<8u>(R, tid, 0u);
   __syncthreads();
 
   // --------------------------- 3. inner sweeps ----------------------------
   int definite;
   unsigned npos;
-  if (P.gdefinite) {
-    definite = P.gdefinite;
-    npos = 0u;
-  }
-  else { // block-local signature (share/device_code_nosort_solveV.hpp:33-67)
-    const unsigned ifc0 = iBlk * kNColB, ifc1 = jBlk * kNColB, nplus = P.nplus;
-    if (nplus <= ifc0) {
-      npos = 0u;
-      definite = -1;
-    }
-    else if (nplus <= ifc0 + kNColB) {
-      npos = nplus - ifc0;
-      definite = 0;
-    }
-    else if (nplus <= ifc1) {
-      npos = kNColB;
-      definite = 0;
-    }
-    else if (nplus <= ifc1 + kNColB) {
-      npos = kNColB + (nplus - ifc1);
-      definite = 0;
-    }
-    else {
-      npos = 2u * kNColB;
-      definite = +1;
-    }
-  }
+  block_signature(P, iBlk, jBlk, definite, npos);
   unsigned blk_s, blk_b;
-  inner_sweeps<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, lane, warp, blk_s, blk_b);
+  inner_sweeps<SORT, 8u>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, lane, warp, 0u, blk_s, blk_b);
 
-  if (rank == 0u && tid == 0u && blk_s) {
-    if (blk_b)
-      atomicAdd(P.cvg, (((unsigned long long)blk_b) << 32) | blk_s);
-    else
-      atomicAdd(reinterpret_cast<unsigned *>(P.cvg), blk_s); // low word, as the reference
-  }
+  if (rank == 0u && tid == 0u)
+    add_counts(P, blk_s, blk_b);
   if (!SORT && !blk_s) { // no rotation: the block pair is unchanged
     if (tid == 0u && nmine > 0u && !mbar_wait_bounded(&bars[4u], 0u, kWaitLimit))
       atomicOr(P.err, kErrWaitTimeout); // the prefetched copy has landed before we leave
@@ -682,26 +871,7 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
       stage_geom(rank + i * NSPLIT, ci, cj, ld, base, rows);
       double acc[4][8]; // the whole warp computes (rows past the end: discarded)
       update_stage(stg + (i % kUpdStages) * kUpdStage, VT, rg, sub, cg8, acc);
-      // lanes l and l^8 own the same 4 rows of column groups 2h and 2h+1:
-      // they trade halves so that each store instruction fills whole 32-byte
-      // sectors (rows r0..r0+1 from the even lane, r0+2..r0+3 from the odd
-      // one, same column)
-      const bool live = sub * 32u < rows;
-      const unsigned r0 = base + sub * 32u + rg * 4u;
-      const bool even = !(cg8 & 1u);
-      const unsigned ce = (cg8 & ~1u) * 8u, roff = even ? 0u : 2u;
-#pragma unroll
-      for (unsigned v = 0u; v < 8u; ++v) {
-        const double s0v = even ? acc[2][v] : acc[0][v], s1v = even ? acc[3][v] : acc[1][v];
-        const double r0v = __shfl_xor_sync(0xffffffffu, s0v, 8), r1v = __shfl_xor_sync(0xffffffffu, s1v, 8);
-        if (live) {
-          const unsigned c1 = ce + v, c2 = ce + 8u + v;
-          double *const col1 = ((c1 < 16u) ? (ci + (size_t)c1 * ld) : (cj + (size_t)(c1 - 16u) * ld)) + r0 + roff;
-          double *const col2 = ((c2 < 16u) ? (ci + (size_t)c2 * ld) : (cj + (size_t)(c2 - 16u) * ld)) + r0 + roff;
-          *reinterpret_cast<double2 *>(col1) = even ? make_double2(acc[0][v], acc[1][v]) : make_double2(r0v, r1v);
-          *reinterpret_cast<double2 *>(col2) = even ? make_double2(r0v, r1v) : make_double2(acc[2][v], acc[3][v]);
-        }
-      }
+      update_store(acc, ci, cj, ld, base, rows, rg, sub, cg8);
     }
     if (__syncthreads_or(fail)) { // uniform decision; drain (bounded), report
       if (warp == 0u && lane == 0u) {
@@ -710,6 +880,237 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
           (void)mbar_wait_bounded(&bars[4u + ((i + 1u) % kUpdStages)], ((i + 1u) / kUpdStages) & 1u,
                                   kWaitLimit / 8);
         atomicOr(P.err, kErrWaitTimeout);
+      }
+      return;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Two block pairs in one CTA (batched form; pair A of matrix PA, pair B of
+// matrix PB).  The Grams and the updates run on all 8 warps, A's then B's,
+// as one stream of stages each (the copies of B's first stages overlap A's
+// last ones).  The Cholesky factorisations and the inner sweeps, chains of
+// dependent divides and square roots that leave the SM's pipes mostly idle,
+// run concurrently: warps 0-3 take pair A (named barrier 1), warps 4-7 pair B
+// (barrier 2).  Every entry of R, V_loc and the updated columns is computed
+// with the same operations in the same order as by pair_step, so each matrix
+// gets the bits it would get alone.
+// ---------------------------------------------------------------------------
+constexpr unsigned kOffR2 = kSmemDoubles; // pair B's R (later B^T), V_loc, counters
+constexpr unsigned kOffVl2 = kOffR2 + 32u * kVTLd;
+constexpr unsigned kOffRed2 = kOffVl2 + 1024u;
+constexpr unsigned kSmemDoubles2 = kOffRed2 + 16u;
+
+size_t batch2_smem_bytes() { return (size_t)kSmemDoubles2 * sizeof(double); }
+
+template <bool SORT, bool ACCV>
+__device__ __forceinline__ void pair_step2(const StepParams &PA, const unsigned stepA, const unsigned pairA,
+                                           const StepParams &PB, const unsigned stepB, const unsigned pairB,
+                                           double *const sm)
+{
+  double *const stg = sm;
+  uint8_t *const s0 = reinterpret_cast<uint8_t *>(sm + kOffS0);
+  uint64_t *const bars = reinterpret_cast<uint64_t *>(sm + kOffBar);
+  unsigned *const flags = reinterpret_cast<unsigned *>(sm + kOffRed2) + 30u; // [g]: pair g updates
+
+  const unsigned tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+  size_t pidx = ((size_t)stepA * PA.pairs + pairA) * 2u;
+  const unsigned iA = PA.strat1[pidx + 0u], jA = PA.strat1[pidx + 1u];
+  pidx = ((size_t)stepB * PB.pairs + pairB) * 2u;
+  const unsigned iB = PB.strat1[pidx + 0u], jB = PB.strat1[pidx + 1u];
+
+  for (unsigned i = tid; i < 256u; i += kThreads)
+    reinterpret_cast<uint32_t *>(s0)[i] = reinterpret_cast<const uint32_t *>(PA.strat0)[i];
+  if (tid == 0u) {
+    for (unsigned b = 0u; b < 8u; ++b)
+      mbar_init(&bars[b], 1u);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  // ------------------------------ 1. Grams --------------------------------
+  // stages 0 .. ngA-1 are A's, ngA .. ngA+ngB-1 B's
+  const unsigned ntA = PA.nrow >> 6, ntB = PB.nrow >> 6;
+  const unsigned ngA = (ntA + kGramTiles - 1u) / kGramTiles, ngB = (ntB + kGramTiles - 1u) / kGramTiles;
+  const unsigned ng = ngA + ngB;
+  unsigned gx0 = 0u, gy = 0u;
+  const bool gthr = gram_lane_of<1u>(0u, warp, lane, gx0, gy);
+  double gacc[4] = {+0.0, +0.0, +0.0, +0.0};
+  auto stage_tiles = [&](const unsigned k) {
+    return (k < ngA) ? min(kGramTiles, ntA - k * kGramTiles) : min(kGramTiles, ntB - (k - ngA) * kGramTiles);
+  };
+  auto issue_gram = [&](const unsigned k) {
+    const unsigned s = k % kGramStages;
+    const bool a = k < ngA;
+    const unsigned t0 = (a ? k : (k - ngA)) * kGramTiles, nt = stage_tiles(k);
+    const CUtensorMap *const tm = a ? &PA.tmGram : &PB.tmGram;
+    const int ci = (int)((a ? iA : iB) * kNColB), cj = (int)((a ? jA : jB) * kNColB);
+    double *const st = stg + s * kGramStage;
+    mbar_arrive_expect_tx(&bars[s], nt * 2u * kGramBoxBytes);
+    for (unsigned t = 0u; t < nt; ++t) {
+      tma_load_4d(st + t * kGramTileLd, tm, 0, 0, (int)(t0 + t), ci, &bars[s]);
+      tma_load_4d(st + t * kGramTileLd + 16u * kGramColLd, tm, 0, 0, (int)(t0 + t), cj, &bars[s]);
+    }
+  };
+  auto put_gram = [&](double *const R) { // our share of the lower triangle
+    if (gthr) {
+#pragma unroll
+      for (unsigned u = 0u; u < 4u; ++u) {
+        if (gx0 + u >= gy)
+          R[gy * 32u + gx0 + u] = gacc[u];
+        gacc[u] = +0.0;
+      }
+    }
+  };
+
+  if (tid == 0u)
+    for (unsigned k = 0u; k + 1u < kGramStages && k < ng; ++k)
+      issue_gram(k);
+  unsigned k = 0u;
+  int failed = 0;
+  for (; k < ng; ++k) {
+    if (tid == 0u && k + kGramStages - 1u < ng)
+      issue_gram(k + kGramStages - 1u);
+    int fail = 0;
+    if (warp < 5u) {
+      if (!mbar_wait_bounded(&bars[k % kGramStages], (k / kGramStages) & 1u, kWaitLimit))
+        fail = 1;
+      else if (gthr) {
+        const unsigned nt = stage_tiles(k);
+        for (unsigned t = 0u; t < nt; ++t)
+          gram_tile(stg + (k % kGramStages) * kGramStage, t * kGramTileLd, gx0, gy, gacc);
+      }
+      if (k + 1u == ngA)
+        put_gram(sm + kOffR);
+      else if (k + 1u == ng)
+        put_gram(sm + kOffR2);
+    }
+    failed = __syncthreads_or(fail);
+    if (failed)
+      break;
+  }
+  if (failed) {
+    if (tid == 0u) {
+      for (unsigned q = k; q < ng && q < k + kGramStages; ++q)
+        (void)mbar_wait_bounded(&bars[q % kGramStages], (q / kGramStages) & 1u, kWaitLimit / 8);
+      atomicOr(PA.err, kErrWaitTimeout);
+      atomicOr(PB.err, kErrWaitTimeout);
+    }
+    return;
+  }
+
+  // A's first update stage, in flight during the serial phases
+  const unsigned nGA = (PA.nrow + kUpdRows - 1u) / kUpdRows, nGB = (PB.nrow + kUpdRows - 1u) / kUpdRows;
+  const unsigned nstA = nGA + (ACCV ? (PA.ncol + kUpdRows - 1u) / kUpdRows : 0u);
+  const unsigned nstB = nGB + (ACCV ? (PB.ncol + kUpdRows - 1u) / kUpdRows : 0u);
+  // update stage geometry: pair g's i-th stage
+  auto stage_geom = [&](const unsigned g, const unsigned i, double *&ci, double *&cj, size_t &ld, unsigned &base,
+                        unsigned &rows, const CUtensorMap *&tm, int &piece) {
+    const StepParams &P = g ? PB : PA;
+    const unsigned nG = g ? nGB : nGA, iBlk = g ? iB : iA, jBlk = g ? jB : jA;
+    if (i < nG) {
+      ci = P.G + (size_t)iBlk * kNColB * P.ldG;
+      cj = P.G + (size_t)jBlk * kNColB * P.ldG;
+      ld = P.ldG;
+      base = i * kUpdRows;
+      rows = min(kUpdRows, P.nrow - base);
+      tm = &P.tmG;
+    }
+    else {
+      ci = P.V + (size_t)iBlk * kNColB * P.ldV;
+      cj = P.V + (size_t)jBlk * kNColB * P.ldV;
+      ld = P.ldV;
+      base = (i - nG) * kUpdRows;
+      rows = min(kUpdRows, P.ncol - base);
+      tm = &P.tmV;
+    }
+    piece = (int)(base >> 5);
+  };
+  auto issue_upd = [&](const unsigned q, const unsigned g, const unsigned i) { // stream position q
+    double *ci, *cj;
+    size_t ld;
+    unsigned base, rows;
+    const CUtensorMap *tm;
+    int piece;
+    stage_geom(g, i, ci, cj, ld, base, rows, tm, piece);
+    const unsigned s = q % kUpdStages;
+    double *const st = stg + s * kUpdStage;
+    mbar_arrive_expect_tx(&bars[4u + s], 2u * kUpdBoxBytes);
+    tma_load_3d(st, tm, 0, piece, (int)((g ? iB : iA) * kNColB), &bars[4u + s]);
+    tma_load_3d(st + 16u * kUpdColLd, tm, 0, piece, (int)((g ? jB : jA) * kNColB), &bars[4u + s]);
+  };
+  if (tid == 0u)
+    issue_upd(0u, 0u, 0u);
+
+  // ------------------- 2.-3. Cholesky and inner sweeps --------------------
+  {
+    const unsigned grp = warp >> 2, gt = tid & 127u, gw = warp & 3u;
+    const StepParams &P = grp ? PB : PA;
+    double *const R = sm + (grp ? kOffR2 : kOffR);
+    double *const Vl = sm + (grp ? kOffVl2 : kOffVl);
+    unsigned *const red = reinterpret_cast<unsigned *>(sm + (grp ? kOffRed2 : kOffRed));
+    for (unsigned i = gt; i < 1024u; i += 128u)
+      Vl[i] = ((i >> 5) == (i & 31u)) ? 1.0 : 0.0;
+    chol32_grp<4u>(R, gt, 1u + grp);
+    bar_sync(1u + grp, 128u);
+    int definite;
+    unsigned npos;
+    block_signature(P, grp ? iB : iA, grp ? jB : jA, definite, npos);
+    unsigned blk_s, blk_b;
+    inner_sweeps_q<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, lane, gw, 1u + grp, blk_s, blk_b);
+    if (gt == 0u) {
+      add_counts(P, blk_s, blk_b);
+      flags[grp] = (SORT || blk_s) ? 1u : 0u;
+    }
+  }
+  __syncthreads();
+  const bool updA = flags[0] != 0u, updB = flags[1] != 0u;
+  // the stream of update stages: A's (or, when A is unchanged, its prefetched
+  // first stage, waited for and dropped), then B's
+  const unsigned qa = updA ? nstA : 1u, nq = qa + (updB ? nstB : 0u);
+  if (nq == 1u && !updA) {
+    if (tid == 0u && !mbar_wait_bounded(&bars[4u], 0u, kWaitLimit))
+      atomicOr(PA.err, kErrWaitTimeout);
+    return;
+  }
+
+  // ------------------------------ 4. updates ------------------------------
+  for (unsigned i = tid; i < 2048u; i += kThreads) { // both R are dead: B^T[s][c] = V_loc[s][c]
+    const unsigned g = i >> 10, c = (i >> 5) & 31u, s_ = i & 31u;
+    (sm + (g ? kOffR2 : kOffR))[s_ * kVTLd + c] = E32(sm + (g ? kOffVl2 : kOffVl), s_, c);
+  }
+  __syncthreads();
+  const unsigned rg = warp, sub = lane & 7u, cg8 = lane >> 3;
+  for (unsigned q = 0u; q < nq; ++q) {
+    if (tid == 0u && q + 1u < nq) {
+      const unsigned q1 = q + 1u;
+      if (q1 < qa)
+        issue_upd(q1, 0u, q1);
+      else
+        issue_upd(q1, 1u, q1 - qa);
+    }
+    const int fail = !__all_sync(0xffffffffu, mbar_wait_bounded(&bars[4u + (q % kUpdStages)], (q / kUpdStages) & 1u,
+                                                                kWaitLimit));
+    const unsigned g = (q < qa) ? 0u : 1u;
+    if (!fail && (g == 1u || updA)) {
+      double *ci, *cj;
+      size_t ld;
+      unsigned base, rows;
+      const CUtensorMap *tm;
+      int piece;
+      stage_geom(g, g ? q - qa : q, ci, cj, ld, base, rows, tm, piece);
+      double acc[4][8];
+      update_stage(stg + (q % kUpdStages) * kUpdStage, sm + (g ? kOffR2 : kOffR), rg, sub, cg8, acc);
+      update_store(acc, ci, cj, ld, base, rows, rg, sub, cg8);
+    }
+    if (__syncthreads_or(fail)) {
+      if (tid == 0u) {
+        (void)mbar_wait_bounded(&bars[4u + (q % kUpdStages)], (q / kUpdStages) & 1u, kWaitLimit / 8);
+        if (q + 1u < nq)
+          (void)mbar_wait_bounded(&bars[4u + ((q + 1u) % kUpdStages)], ((q + 1u) / kUpdStages) & 1u,
+                                  kWaitLimit / 8);
+        atomicOr(g ? PB.err : PA.err, kErrWaitTimeout);
       }
       return;
     }
@@ -802,13 +1203,13 @@ __global__ void __launch_bounds__(kThreads, 1) l1_sweep_kernel(const __grid_cons
 // outer step of its own sweep (matrix b: step kstep[b] mod steps1), so small
 // matrices run their short sweeps back to back while large ones progress.  A
 // persistent grid (one CTA per SM) takes the block pairs -- (matrix << 16) |
-// pair, largest matrices first -- from a work queue; each is processed by
-// pair_step exactly as in the single-matrix launch with one CTA per pair, so
-// every matrix gets the bits it would get alone.  Converged matrices are
-// skipped.  The mbarriers are invalidated after each pair (pair_step
-// initialises them).
+// pair, largest matrices first -- from a work queue, W at a time: with W = 2
+// two live pairs go through pair_step2 together, a lone one through
+// pair_step with one CTA, so every matrix gets the bits it would get alone.
+// Converged matrices are skipped.  The mbarriers are invalidated after each
+// item (both step forms initialise them).
 // ---------------------------------------------------------------------------
-template <bool SORT, bool ACCV>
+template <bool SORT, bool ACCV, unsigned W>
 __global__ void __launch_bounds__(kThreads, 1) l1_batch_kernel(const __grid_constant__ BatchStep B)
 {
   extern __shared__ __align__(128) double sm[];
@@ -816,19 +1217,45 @@ __global__ void __launch_bounds__(kThreads, 1) l1_batch_kernel(const __grid_cons
   uint64_t *const bars = reinterpret_cast<uint64_t *>(sm + kOffBar);
   for (;;) {
     if (threadIdx.x == 0u)
-      item = atomicAdd(B.queue, 1u);
+      item = atomicAdd(B.queue, W);
     __syncthreads();
     const unsigned it = item;
     const bool stop = (it >= B.nitems) || (*(volatile int *)B.err != 0);
     __syncthreads(); // every thread has read item
     if (stop)
       break;
-    const uint32_t e = B.items[it];
-    const unsigned b = e >> 16u, pair = e & 0xffffu;
-    if (B.done[b])
+    const uint32_t e0 = B.items[it];
+    const unsigned b0 = e0 >> 16u;
+    const bool live0 = !B.done[b0];
+    uint32_t e1 = 0u;
+    bool live1 = false;
+    if (W == 2u && it + 1u < B.nitems) {
+      e1 = B.items[it + 1u];
+      live1 = !B.done[e1 >> 16u];
+    }
+    if (!live0 && !live1)
       continue;
-    const BatchMat &m = B.mats[b];
-    pair_step<SORT, ACCV, 1u>(m.p, B.kstep[b] % m.steps1, pair, 0u, sm);
+    if (live0 && live1 && B.mats[b0].p.strat0 == B.mats[e1 >> 16u].p.strat0) {
+      const BatchMat &ma = B.mats[b0], &mb = B.mats[e1 >> 16u];
+      pair_step2<SORT, ACCV>(ma.p, B.kstep[b0] % ma.steps1, e0 & 0xffffu, mb.p, B.kstep[e1 >> 16u] % mb.steps1,
+                             e1 & 0xffffu, sm);
+    }
+    else {
+      for (unsigned h = 0u; h < 2u; ++h) {
+        const bool live = h ? live1 : live0;
+        if (!live)
+          continue;
+        const uint32_t e = h ? e1 : e0;
+        const BatchMat &m = B.mats[e >> 16u];
+        pair_step<SORT, ACCV, 1u>(m.p, B.kstep[e >> 16u] % m.steps1, e & 0xffffu, 0u, sm);
+        __syncthreads();
+        if (threadIdx.x == 0u)
+          for (unsigned k = 0u; k < 8u; ++k)
+            mbar_inval(&bars[k]);
+        __syncthreads();
+      }
+      continue;
+    }
     __syncthreads();
     if (threadIdx.x == 0u)
       for (unsigned k = 0u; k < 8u; ++k)
@@ -1066,35 +1493,47 @@ template <bool S, bool A, unsigned N> static cudaError_t launch(const StepParams
   return cudaLaunchKernelEx(&cfg, l1_step_kernel<S, A, N>, p);
 }
 
-template <bool S, bool A> static cudaError_t set_smem_batch(const int bytes)
+template <bool S, bool A> static cudaError_t set_smem_batch()
 {
-  return cudaFuncSetAttribute(l1_batch_kernel<S, A>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaError_t e = cudaFuncSetAttribute(l1_batch_kernel<S, A, 1u>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)l1_smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(l1_batch_kernel<S, A, 2u>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)batch2_smem_bytes());
+  return e;
 }
 
 cudaError_t batch_configure()
 {
-  const int b = (int)l1_smem_bytes();
   cudaError_t e;
-  if ((e = set_smem_batch<false, false>(b)) || (e = set_smem_batch<false, true>(b)) ||
-      (e = set_smem_batch<true, false>(b)) || (e = set_smem_batch<true, true>(b)))
+  if ((e = set_smem_batch<false, false>()) || (e = set_smem_batch<false, true>()) ||
+      (e = set_smem_batch<true, false>()) || (e = set_smem_batch<true, true>()))
     return e;
   return cudaSuccess;
 }
 
-cudaError_t launch_batch_step(const bool sort, const bool accv, const BatchStep &b, const unsigned ctas,
-                              cudaStream_t s)
+template <bool S, bool A>
+static void batch_launch(const unsigned width, const BatchStep &b, const unsigned ctas, cudaStream_t s)
 {
-  const size_t sm = l1_smem_bytes();
+  if (width == 2u)
+    l1_batch_kernel<S, A, 2u><<<ctas, kThreads, batch2_smem_bytes(), s>>>(b);
+  else
+    l1_batch_kernel<S, A, 1u><<<ctas, kThreads, l1_smem_bytes(), s>>>(b);
+}
+
+cudaError_t launch_batch_step(const bool sort, const bool accv, const unsigned width, const BatchStep &b,
+                              const unsigned ctas, cudaStream_t s)
+{
   if (sort) {
     if (accv)
-      l1_batch_kernel<true, true><<<ctas, kThreads, sm, s>>>(b);
+      batch_launch<true, true>(width, b, ctas, s);
     else
-      l1_batch_kernel<true, false><<<ctas, kThreads, sm, s>>>(b);
+      batch_launch<true, false>(width, b, ctas, s);
   }
   else if (accv)
-    l1_batch_kernel<false, true><<<ctas, kThreads, sm, s>>>(b);
+    batch_launch<false, true>(width, b, ctas, s);
   else
-    l1_batch_kernel<false, false><<<ctas, kThreads, sm, s>>>(b);
+    batch_launch<false, false>(width, b, ctas, s);
   return cudaGetLastError();
 }
 

@@ -107,6 +107,12 @@ void gjx_set_sweep_mode(int mode);
  * for the automatic choice.  The results are the same bits for any value. */
 void gjx_set_split(unsigned n);
 
+/* Block pairs that a CTA of the batched form (gjx_hypJacL2_batched) takes
+ * at a time: 2 (default; the Cholesky factorisations and inner sweeps of the
+ * two run concurrently on two groups of 4 warps) or 1.  The results are the
+ * same bits for either value. */
+void gjx_set_batch_width(unsigned w);
+
 /*
  * Autotuner: time every launch configuration of this shape -- 1, 2 or 4
  * CTAs per block pair (where the pairs fit), one launch per outer step or

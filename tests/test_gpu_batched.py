@@ -2,7 +2,7 @@
 exactly what the single-matrix device call gives it -- U, V, D bit for bit,
 sweeps and rotation counts -- for mixed sizes (64..512 columns, square and
 tall), mixed signatures (J = I, J = -I, mixed), all four kernel variants
-(ALG 3, 9, 11, 1), and a matrix with invalid arguments that is reported and
+(ALG 3, 9, 11, 1), one and two block pairs per CTA, and a matrix with invalid arguments that is reported and
 left alone while the others run."""
 
 import numpy as np
@@ -29,10 +29,12 @@ CASES = [(64, 64, 64), (128, 128, 64), (192, 192, 0), (256, 256, 256), (320, 320
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("width", [2, 1])
 @pytest.mark.parametrize("alg", [11, 9, 3, 1])
-def test_batched_equals_single(built, alg):
+def test_batched_equals_single(built, alg, width):
     import torch
     import gpujachx_b200 as g
+    g.lib().gjx_set_batch_width(width)   # 2: two block pairs per CTA, from different matrices too
     g.init_strats(None, "cycwor", 32, "cycwor", 4)   # the family; each matrix takes its own n1 table
     full = bool(alg & 2)
     mats = []
@@ -43,6 +45,7 @@ def test_batched_equals_single(built, alg):
     batch = [_dev(G, full) for G, _ in mats]
     res = g.hypJacL2_batched(alg, [b[0] for b in batch], [p for _, p in mats], Vs=[b[1] for b in batch] if full else None,
                              Ds=[b[2] for b in batch])
+    g.lib().gjx_set_batch_width(2)
     assert res.info == [0] * len(mats)
     for k, (G, p) in enumerate(mats):
         n = G.shape[1]
