@@ -16,7 +16,7 @@ constexpr unsigned kNSweep = 30u; // outer and full-block inner sweep cap (share
 struct alignas(64) StepParams {
   CUtensorMap tmG;              // 3-D view (32 rows, nrow/32 pieces, ncol columns) of G
   CUtensorMap tmV;              // the same of V (ACCV only)
-  CUtensorMap tmGram;           // 4-D view (32 rows, 2 pieces, nrow/64 tiles, ncol columns) of G
+  CUtensorMap tmGram;           // 3-D view (64 rows, nrow/64 tiles, ncol columns) of G
   double *G;                    // nrow x ncol, column major, leading dim ldG
   double *V;                    // ncol x ncol, leading dim ldV (ACCV only)
   const uint16_t *strat1;       // [steps1][pairs][2] block pairs (outer level)

@@ -48,20 +48,19 @@ constexpr unsigned kThreads = 256u;
 constexpr long long kWaitLimit = 2000000000ll; // ~1 s of cycles per wait
 
 // Gram staging: a stage holds 2 tiles of 64 rows of the 32 columns, brought
-// in by the TMA engine: per tile and block one box {34 rows, 3 pieces, 1 tile,
-// 16 columns} of the 4-D view (32 rows, 2 pieces, tiles, columns) of G.  Rows
-// 32-33 of a piece and the third piece lie outside the view and are
-// zero-filled, so column c of a tile starts at c * 102 and tile row r sits at
-// r + 2 (r >> 5).  The column stride of 102 doubles (51 16-byte granules, odd)
-// puts the row pairs of 8 consecutive columns in 8 bank groups.  3 stages in
-// flight.
+// in by the TMA engine: per tile and block one box {66 rows, 1 tile, 16
+// columns} of the 3-D view (64 rows, tiles, columns) of G.  Rows 64-65 lie
+// outside the view and are zero-filled, so column c of a tile starts at
+// c * 66.  The column stride of 66 doubles (33 16-byte granules, odd) puts the
+// row pairs of 8 consecutive columns in 8 bank groups.  4 stages in flight;
+// the copies are issued by a thread of warp 7, which computes no Gram entry.
 constexpr unsigned kGramTiles = 2u;
-constexpr unsigned kGramStages = 3u;
-constexpr unsigned kGramColLd = 102u;
+constexpr unsigned kGramStages = 4u;
+constexpr unsigned kGramColLd = 66u;
 constexpr unsigned kGramTileLd = 32u * kGramColLd;
 constexpr unsigned kGramStage = kGramTiles * kGramTileLd; // doubles
-constexpr uint32_t kGramBoxBytes = 34u * 3u * 16u * 8u;
-__device__ __forceinline__ unsigned grow(const unsigned r) { return r + 2u * (r >> 5); }
+constexpr uint32_t kGramBoxBytes = 66u * 16u * 8u;
+constexpr unsigned kIssuer = 224u; // lane 0 of warp 7
 
 // Update staging: 256 rows x 32 columns; the 32-row piece p of column c
 // starts at c*272 + p*34 (2 doubles of skew per piece spread the banks).
@@ -114,7 +113,7 @@ __device__ __forceinline__ void gram_tile(const double *const st, const unsigned
   double2 Yb[3], Xb[3][4];
 #pragma unroll
   for (unsigned q = 0u; q < 2u; ++q) {
-    const unsigned o = grow((x0 + 2u * q) & 63u);
+    const unsigned o = (x0 + 2u * q) & 63u;
     Yb[q] = *reinterpret_cast<const double2 *>(yp + o);
 #pragma unroll
     for (unsigned u = 0u; u < 4u; ++u)
@@ -124,7 +123,7 @@ __device__ __forceinline__ void gram_tile(const double *const st, const unsigned
   for (unsigned kp = 0u; kp < 34u; ++kp) { // pairs k = 2kp, 2kp + 1
     if (kp + 2u < 34u) {
       const unsigned q = (kp + 2u) % 3u;
-      const unsigned o = grow((x0 + 2u * (kp + 2u)) & 63u);
+      const unsigned o = (x0 + 2u * (kp + 2u)) & 63u;
       Yb[q] = *reinterpret_cast<const double2 *>(yp + o);
 #pragma unroll
       for (unsigned u = 0u; u < 4u; ++u)
@@ -735,18 +734,18 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
     mbar_arrive_expect_tx(&bars[s], nt * 2u * kGramBoxBytes);
     for (unsigned t = 0u; t < nt; ++t) {
       const int tile = (int)(k * kGramTiles + t);
-      tma_load_4d(st + t * kGramTileLd, &P.tmGram, 0, 0, tile, (int)(iBlk * kNColB), &bars[s]);
-      tma_load_4d(st + t * kGramTileLd + 16u * kGramColLd, &P.tmGram, 0, 0, tile, (int)(jBlk * kNColB), &bars[s]);
+      tma_load_3d(st + t * kGramTileLd, &P.tmGram, 0, tile, (int)(iBlk * kNColB), &bars[s]);
+      tma_load_3d(st + t * kGramTileLd + 16u * kGramColLd, &P.tmGram, 0, tile, (int)(jBlk * kNColB), &bars[s]);
     }
   };
 
-  if (tid == 0u)
+  if (tid == kIssuer)
     for (unsigned k = 0u; k + 1u < kGramStages && k < ngst; ++k)
       issue_gram(k);
   unsigned k = 0u;
   int failed = 0;
   for (; k < ngst; ++k) {
-    if (tid == 0u && k + kGramStages - 1u < ngst)
+    if (tid == kIssuer && k + kGramStages - 1u < ngst)
       issue_gram(k + kGramStages - 1u); // into the buffer released at the end of stage k - 1
     int fail = 0;
     if (warp < gwarps) {
@@ -949,8 +948,8 @@ __device__ __forceinline__ void pair_step2(const StepParams &PA, const unsigned 
     double *const st = stg + s * kGramStage;
     mbar_arrive_expect_tx(&bars[s], nt * 2u * kGramBoxBytes);
     for (unsigned t = 0u; t < nt; ++t) {
-      tma_load_4d(st + t * kGramTileLd, tm, 0, 0, (int)(t0 + t), ci, &bars[s]);
-      tma_load_4d(st + t * kGramTileLd + 16u * kGramColLd, tm, 0, 0, (int)(t0 + t), cj, &bars[s]);
+      tma_load_3d(st + t * kGramTileLd, tm, 0, (int)(t0 + t), ci, &bars[s]);
+      tma_load_3d(st + t * kGramTileLd + 16u * kGramColLd, tm, 0, (int)(t0 + t), cj, &bars[s]);
     }
   };
   auto put_gram = [&](double *const R) { // our share of the lower triangle
@@ -964,13 +963,13 @@ __device__ __forceinline__ void pair_step2(const StepParams &PA, const unsigned 
     }
   };
 
-  if (tid == 0u)
+  if (tid == kIssuer)
     for (unsigned k = 0u; k + 1u < kGramStages && k < ng; ++k)
       issue_gram(k);
   unsigned k = 0u;
   int failed = 0;
   for (; k < ng; ++k) {
-    if (tid == 0u && k + kGramStages - 1u < ng)
+    if (tid == kIssuer && k + kGramStages - 1u < ng)
       issue_gram(k + kGramStages - 1u);
     int fail = 0;
     if (warp < 5u) {
@@ -1447,12 +1446,12 @@ cudaError_t make_gram_map(CUtensorMap *tm, const double *base, const unsigned nr
       return cudaErrorNotSupported;
     encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   }
-  // (rows within a 32-row piece, 2 pieces, 64-row tiles, columns); box {34, 3, 1, 16}
-  const cuuint64_t dims[4] = {32u, 2u, nrow / 64u, ncol};
-  const cuuint64_t strides[3] = {32u * sizeof(double), 64u * sizeof(double), (cuuint64_t)ld * sizeof(double)};
-  const cuuint32_t box[4] = {34u, 3u, 1u, 16u};
-  const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
-  const CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4u, const_cast<double *>(base), dims, strides, box,
+  // (rows within a 64-row tile, tiles, columns); box {66, 1, 16}
+  const cuuint64_t dims[3] = {64u, nrow / 64u, ncol};
+  const cuuint64_t strides[2] = {64u * sizeof(double), (cuuint64_t)ld * sizeof(double)};
+  const cuuint32_t box[3] = {66u, 1u, 16u};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  const CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3u, const_cast<double *>(base), dims, strides, box,
                             estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return (r == CUDA_SUCCESS) ? cudaSuccess : cudaErrorInvalidValue;
