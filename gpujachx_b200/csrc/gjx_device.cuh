@@ -287,13 +287,34 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *tm, co
                : "memory");
 }
 
-__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *tm, const int c0, const int c1,
-                                            const int c2, const int c3, uint64_t *bar)
+// TMA tensor store of a 3-D box of shared memory to (c0, c1, c2) of the
+// tensor map, in this thread's current bulk async-group; elements of the box
+// outside the tensor are not written.  c0 = 0 here; no coordinate is negative.
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap *tm, const void *src, const int c0, const int c1,
+                                             const int c2)
 {
-  asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-               "%5}], [%6];" ::"r"(smem_u32(dst)),
-               "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
+                   reinterpret_cast<uint64_t>(tm)),
+               "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2)
                : "memory");
 }
+
+// close this thread's bulk async-group
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+// this thread's bulk groups have finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
+// this thread's bulk groups are complete (their global writes performed),
+// and ordered before this thread's later generic-proxy operations
+__device__ __forceinline__ void bulk_wait_all()
+{
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+// this thread's shared-memory writes become visible to the async proxy (a TMA
+// store issued after a barrier)
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 } // namespace gjx

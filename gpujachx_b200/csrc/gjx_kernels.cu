@@ -7,7 +7,7 @@
 //   1. Gram matrix of the M x 32 column pair [G_i G_j], lower triangle only
 //      (the Cholesky never reads the upper one).  Each CTA streams the whole
 //      pair through shared memory in 64-row tiles (TMA tensor copies into a
-//      bank-skewed, zero-padded layout, mbarrier completion, 3 stages of 2
+//      bank-skewed, zero-padded layout, mbarrier completion, 4 stages of 2
 //      tiles) and computes its share of the 528 entries; every
 //      entry is one FMA chain in the reference's row order
 //      (share/device_code_common_Cholesky.hpp:4-56).  A lane holds the 4
@@ -31,7 +31,8 @@
 //      cluster (the first one in flight during steps 2 and 3); each output
 //      is a 32-FMA chain in the reference's skewed order
 //      (share/device_code_common.hpp:146-185), computed in 4x8 register
-//      tiles along anti-diagonals, stored as full 32-byte sectors.
+//      tiles along anti-diagonals, put back in place of the stage's operands
+//      and written out by TMA tensor stores that overlap the next stage.
 //
 // All arithmetic is in the reference's order, so results are bit-identical.
 #include <cooperative_groups.h>
@@ -617,30 +618,20 @@ __device__ __forceinline__ void update_stage(const double *const st, const doubl
   }
 }
 
-// stores of one stage's tile: lanes l and l^8 own the same 4 rows of column
-// groups 2h and 2h+1; they trade halves so that each store instruction fills
-// whole 32-byte sectors (rows r0..r0+1 from the even lane, r0+2..r0+3 from
-// the odd one, same column).  Rows past the end (a stage of rows < 256) are
-// not stored.
-__device__ __forceinline__ void update_store(const double (&acc)[4][8], double *const ci, double *const cj,
-                                             const size_t ld, const unsigned base, const unsigned rows,
-                                             const unsigned rg, const unsigned sub, const unsigned cg8)
+// the stage's results in place of its operands: the thread's 4 rows x 8
+// columns go where update_stage read them; warp rg read only its own rows
+// (rg*4 .. rg*4+3 of each 32-row piece), so after __syncwarp nothing that
+// another lane still needs is overwritten.  A TMA store then writes the stage
+// back (rows 32-33 of a piece lie outside the view and are not written).
+__device__ __forceinline__ void update_put(double *const st, const double (&acc)[4][8], const unsigned rg,
+                                           const unsigned sub, const unsigned cg8)
 {
-  const bool live = sub * 32u < rows;
-  const unsigned r0 = base + sub * 32u + rg * 4u;
-  const bool even = !(cg8 & 1u);
-  const unsigned ce = (cg8 & ~1u) * 8u, roff = even ? 0u : 2u;
+  double *const o = st + sub * 34u + rg * 4u;
 #pragma unroll
   for (unsigned v = 0u; v < 8u; ++v) {
-    const double s0v = even ? acc[2][v] : acc[0][v], s1v = even ? acc[3][v] : acc[1][v];
-    const double r0v = __shfl_xor_sync(0xffffffffu, s0v, 8), r1v = __shfl_xor_sync(0xffffffffu, s1v, 8);
-    if (live) {
-      const unsigned c1 = ce + v, c2 = ce + 8u + v;
-      double *const col1 = ((c1 < 16u) ? (ci + (size_t)c1 * ld) : (cj + (size_t)(c1 - 16u) * ld)) + r0 + roff;
-      double *const col2 = ((c2 < 16u) ? (ci + (size_t)c2 * ld) : (cj + (size_t)(c2 - 16u) * ld)) + r0 + roff;
-      *reinterpret_cast<double2 *>(col1) = even ? make_double2(acc[0][v], acc[1][v]) : make_double2(r0v, r1v);
-      *reinterpret_cast<double2 *>(col2) = even ? make_double2(r0v, r1v) : make_double2(acc[2][v], acc[3][v]);
-    }
+    double *const col = o + (cg8 * 8u + v) * kUpdColLd;
+    *reinterpret_cast<double2 *>(col) = make_double2(acc[0][v], acc[1][v]);
+    *reinterpret_cast<double2 *>(col + 2u) = make_double2(acc[2][v], acc[3][v]);
   }
 }
 
@@ -705,8 +696,6 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
   const unsigned tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
   const size_t pidx = ((size_t)step * P.pairs + pair) * 2u;
   const unsigned iBlk = P.strat1[pidx + 0u], jBlk = P.strat1[pidx + 1u];
-  double *const Gi = P.G + (size_t)iBlk * kNColB * P.ldG;
-  double *const Gj = P.G + (size_t)jBlk * kNColB * P.ldG;
 
   for (unsigned i = tid; i < 256u; i += kThreads)
     reinterpret_cast<uint32_t *>(s0)[i] = reinterpret_cast<const uint32_t *>(P.strat0)[i];
@@ -835,54 +824,51 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
     VT[s * kVTLd + c] = E32(Vl, s, c);
   }
 
-  double *const Vi = ACCV ? (P.V + (size_t)iBlk * kNColB * P.ldV) : nullptr;
-  double *const Vj = ACCV ? (P.V + (size_t)jBlk * kNColB * P.ldV) : nullptr;
-
-  auto stage_geom = [&](const unsigned k, double *&ci, double *&cj, size_t &ld, unsigned &base, unsigned &rows) {
-    if (k < nG) {
-      ci = Gi;
-      cj = Gj;
-      ld = P.ldG;
-      base = k * kUpdRows;
-      rows = min(kUpdRows, P.nrow - base);
-    }
-    else {
-      ci = Vi;
-      cj = Vj;
-      ld = P.ldV;
-      base = (k - nG) * kUpdRows;
-      rows = min(kUpdRows, P.ncol - base);
-    }
-  };
   __syncthreads(); // VT ready
+  // stage i: thread 0 issues the copy of stage i + 1 into the other buffer
+  // once the store of stage i - 1 has read it out; the warps compute stage i
+  // and put the results in place; after the barrier thread 0 stores them
+  // with two tensor copies, which overlap the next stage's arithmetic
   const unsigned rg = warp, sub = lane & 7u, cg8 = lane >> 3;
   for (unsigned i = 0u; i < nmine; ++i) {
-    if (tid == 0u && i + 1u < nmine)
+    if (tid == 0u && i + 1u < nmine) {
+      bulk_wait_read();
       issue_upd(i + 1u);
-    // a warp computes only if all its lanes saw the stage land (the shuffles
-    // below need the whole warp)
+    }
+    // a warp computes only if all its lanes saw the stage land
     const int fail = !__all_sync(0xffffffffu, mbar_wait_bounded(&bars[4u + (i % kUpdStages)], (i / kUpdStages) & 1u,
                                                                 kWaitLimit));
+    double *const sb = stg + (i % kUpdStages) * kUpdStage;
     if (!fail) {
-      double *ci, *cj;
-      size_t ld;
-      unsigned base, rows;
-      stage_geom(rank + i * NSPLIT, ci, cj, ld, base, rows);
-      double acc[4][8]; // the whole warp computes (rows past the end: discarded)
-      update_stage(stg + (i % kUpdStages) * kUpdStage, VT, rg, sub, cg8, acc);
-      update_store(acc, ci, cj, ld, base, rows, rg, sub, cg8);
+      double acc[4][8]; // the whole warp computes (rows past the end: not stored)
+      update_stage(sb, VT, rg, sub, cg8, acc);
+      __syncwarp();
+      update_put(sb, acc, rg, sub, cg8);
+      fence_async_shared();
     }
     if (__syncthreads_or(fail)) { // uniform decision; drain (bounded), report
-      if (warp == 0u && lane == 0u) {
+      if (tid == 0u) {
         (void)mbar_wait_bounded(&bars[4u + (i % kUpdStages)], (i / kUpdStages) & 1u, kWaitLimit / 8);
         if (i + 1u < nmine)
           (void)mbar_wait_bounded(&bars[4u + ((i + 1u) % kUpdStages)], ((i + 1u) / kUpdStages) & 1u,
                                   kWaitLimit / 8);
+        bulk_wait_all();
         atomicOr(P.err, kErrWaitTimeout);
       }
       return;
     }
+    if (tid == 0u) {
+      const unsigned k = rank + i * NSPLIT;
+      const bool isG = k < nG;
+      const CUtensorMap *const tm = isG ? &P.tmG : &P.tmV;
+      const int piece = (int)(((isG ? k : (k - nG)) * kUpdRows) >> 5);
+      tma_store_3d(tm, sb, 0, piece, (int)(iBlk * kNColB));
+      tma_store_3d(tm, sb + 16u * kUpdColLd, 0, piece, (int)(jBlk * kNColB));
+      bulk_commit();
+    }
   }
+  if (tid == 0u)
+    bulk_wait_all(); // the stores are complete before the block pair counts as done
 }
 
 // ---------------------------------------------------------------------------
@@ -1084,6 +1070,7 @@ __device__ __forceinline__ void pair_step2(const StepParams &PA, const unsigned 
   for (unsigned q = 0u; q < nq; ++q) {
     if (tid == 0u && q + 1u < nq) {
       const unsigned q1 = q + 1u;
+      bulk_wait_read(); // the store of stage q - 1 has read the buffer stage q + 1 lands in
       if (q1 < qa)
         issue_upd(q1, 0u, q1);
       else
@@ -1092,16 +1079,14 @@ __device__ __forceinline__ void pair_step2(const StepParams &PA, const unsigned 
     const int fail = !__all_sync(0xffffffffu, mbar_wait_bounded(&bars[4u + (q % kUpdStages)], (q / kUpdStages) & 1u,
                                                                 kWaitLimit));
     const unsigned g = (q < qa) ? 0u : 1u;
-    if (!fail && (g == 1u || updA)) {
-      double *ci, *cj;
-      size_t ld;
-      unsigned base, rows;
-      const CUtensorMap *tm;
-      int piece;
-      stage_geom(g, g ? q - qa : q, ci, cj, ld, base, rows, tm, piece);
+    const bool work = g == 1u || updA;
+    double *const sb = stg + (q % kUpdStages) * kUpdStage;
+    if (!fail && work) {
       double acc[4][8];
-      update_stage(stg + (q % kUpdStages) * kUpdStage, sm + (g ? kOffR2 : kOffR), rg, sub, cg8, acc);
-      update_store(acc, ci, cj, ld, base, rows, rg, sub, cg8);
+      update_stage(sb, sm + (g ? kOffR2 : kOffR), rg, sub, cg8, acc);
+      __syncwarp();
+      update_put(sb, acc, rg, sub, cg8);
+      fence_async_shared();
     }
     if (__syncthreads_or(fail)) {
       if (tid == 0u) {
@@ -1109,11 +1094,25 @@ __device__ __forceinline__ void pair_step2(const StepParams &PA, const unsigned 
         if (q + 1u < nq)
           (void)mbar_wait_bounded(&bars[4u + ((q + 1u) % kUpdStages)], ((q + 1u) / kUpdStages) & 1u,
                                   kWaitLimit / 8);
+        bulk_wait_all();
         atomicOr(g ? PB.err : PA.err, kErrWaitTimeout);
       }
       return;
     }
+    if (tid == 0u && work) {
+      double *ci, *cj;
+      size_t ld;
+      unsigned base, rows;
+      const CUtensorMap *tm;
+      int piece;
+      stage_geom(g, g ? q - qa : q, ci, cj, ld, base, rows, tm, piece);
+      tma_store_3d(tm, sb, 0, piece, (int)((g ? iB : iA) * kNColB));
+      tma_store_3d(tm, sb + 16u * kUpdColLd, 0, piece, (int)((g ? jB : jA) * kNColB));
+      bulk_commit();
+    }
   }
+  if (tid == 0u)
+    bulk_wait_all();
 }
 
 // one launch per outer step: block pair blockIdx.x / NSPLIT, cluster rank
