@@ -492,7 +492,7 @@ def main_batch(args):
     t_s = statistics.median(times) / 1000.0
     hbm, peak_kind = _peaks()
     roof = {"bound": "hbm", "achieved": nbytes / t_s / 1e9, "peak": hbm, "unit": "GB/s",
-            "frac": nbytes / t_s / 1e9 / hbm, "traffic": None, "kernel": "gjx::l1_batch_kernel<true,true>",
+            "frac": nbytes / t_s / 1e9 / hbm, "traffic": None, "kernel": f"gjx::l1_batch_kernel<true,true,{width}>",
             "peak_kind": f"{peak_kind} HBM copy bandwidth",
             "note": "algorithmic bytes of all sweeps run, over the device time of the whole batched call",
             "fp64_tflops": flops / t_s / 1e12, "launches_per_step": prof["launches"] // max(1, args.steps)}
