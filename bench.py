@@ -443,8 +443,8 @@ def main_batch(args):
         G0, offs = batch_inputs(sizes, dev, cfg["seed"] + rank)
     nplus = [int(n) if b % 2 == 0 else int(n) // 2 for b, n in enumerate(sizes)]
     g.init_strats(None, "cycwor", 32, "cycwor", 4)
-    width = 1 if os.environ.get("GJX_BATCH_WIDTH") == "1" else 2  # block pairs per CTA at a time
-    g.lib().gjx_set_batch_width(width)
+    width = 1 if os.environ.get("GJX_PAIRS_PER_CTA") == "1" else 2  # block pairs per CTA at a time
+    g.lib().gjx_set_pairs_per_cta(width)
     dG = torch.empty_like(G0)
     dV = torch.empty_like(G0)
     dD = torch.empty(int(sizes.sum()), dtype=torch.float64, device=dev)

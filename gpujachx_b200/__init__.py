@@ -35,7 +35,7 @@ EXPORTS = ("hypJacL2", "init_strats", "gjx_init_strats", "gjx_strat_info", "gjx_
            "gjx_hypJacL2_dev", "gjx_release_cache", "gjx_set_verbose", "gjx_last_error",
            "gjx_version", "gjx_rsqrt_rn_dev", "gjx_profile", "gjx_profile_read", "gjx_hypJacL2_noalloc",
            "gjx_validate_pairs", "gjx_validate_strats", "gjx_configure_device", "gjx_h5_read", "gjx_h5_write",
-           "gjx_hypJacL2_batched", "gjx_set_sweep_mode", "gjx_set_split", "gjx_set_batch_width", "gjx_autotune",
+           "gjx_hypJacL2_batched", "gjx_set_sweep_mode", "gjx_set_split", "gjx_set_pairs_per_cta", "gjx_autotune",
            "gjx_autotune_clear", "gjx_wait_selftest")
 
 
@@ -106,8 +106,8 @@ def lib() -> ctypes.CDLL:
     L.gjx_autotune_clear.restype = None
     L.gjx_set_split.argtypes = [u]
     L.gjx_set_split.restype = None
-    L.gjx_set_batch_width.argtypes = [u]
-    L.gjx_set_batch_width.restype = None
+    L.gjx_set_pairs_per_cta.argtypes = [u]
+    L.gjx_set_pairs_per_cta.restype = None
     L.gjx_set_sweep_mode.argtypes = [i]
     L.gjx_set_sweep_mode.restype = None
     L.gjx_configure_device.argtypes = [i]

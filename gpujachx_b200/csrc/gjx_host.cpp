@@ -50,7 +50,7 @@ Strat g_strat;
 int g_verbose = 1;
 int g_sweep_mode = -1; // -1 automatic (the tuned choice, else per step), 0 per outer step, 1 one launch per sweep
 unsigned g_split = 0u;  // CTAs per block pair: 0 automatic (the tuned choice, else by the SM count), else 1, 2, 4
-unsigned g_batch_width = 2u; // block pairs a CTA of the batched form takes at a time: 1 or 2
+unsigned g_pairs_per_cta = 0u; // block pairs a CTA takes at a time: 0 automatic, 1, or 2
 
 // the autotuner's choices, by (routine, nrow, ncol, nplus)
 struct TuneKey {
@@ -234,6 +234,12 @@ int run_sweeps_core(const unsigned routine, const unsigned nrow, const unsigned 
   }
   if (g_split && g_split * p.pairs <= 148u * 8u)
     p.split = g_split;
+  // two block pairs per CTA: with 1 CTA per pair, when a step has more pairs
+  // than the GPU has SMs (one wave instead of two), or when asked for
+  int dev = 0, sms = 148;
+  GJX_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  GJX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+  p.width = (p.split == 1u && (g_pairs_per_cta == 2u || (!g_pairs_per_cta && p.pairs > (unsigned)sms))) ? 2u : 1u;
   GJX_CUDA(gjx::make_update_map(&p.tmG, dG, nrow, ncol, lddG), "tensor map of G");
   GJX_CUDA(gjx::make_gram_map(&p.tmGram, dG, nrow, ncol, lddG), "Gram tensor map of G");
   if (full)
@@ -561,7 +567,7 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
   const gjx::BatchSweep sw{d_mats, d_ks, d_cvg, d_done, d_swp, d_gs, d_gb, d_q, d_act, nmat};
   const unsigned ctas = std::min<unsigned>((unsigned)sms, (unsigned)items.size());
   for (unsigned k = 0u; k < kLaunches && ce == cudaSuccess; ++k) {
-    ce = gjx::launch_batch_step(cdsort, full, g_batch_width, bs, ctas, st);
+    ce = gjx::launch_batch_step(cdsort, full, (g_pairs_per_cta == 1u) ? 1u : 2u, bs, ctas, st);
     if (ce == cudaSuccess)
       ce = cudaMemsetAsync(d_act, 0, 4u, st); // the count of the last launch is the one read
     if (ce == cudaSuccess)
@@ -1076,10 +1082,10 @@ void gjx_set_split(const unsigned n)
   g_split = (n == 1u || n == 2u || n == 4u) ? n : 0u;
 }
 
-void gjx_set_batch_width(const unsigned w)
+void gjx_set_pairs_per_cta(const unsigned w)
 {
   std::lock_guard<std::mutex> lk(g_mtx);
-  g_batch_width = (w == 1u) ? 1u : 2u;
+  g_pairs_per_cta = (w == 1u || w == 2u) ? w : 0u;
 }
 
 int gjx_autotune(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,

@@ -29,7 +29,8 @@ struct alignas(64) StepParams {
   unsigned s0steps;             // inner steps (31, or 32 for mmstep)
   unsigned nswp0;               // inner sweeps per block pair (1 or 30)
   int gdefinite;                // +1 J = I, -1 J = -I, 0 mixed signs
-  unsigned split;               // CTAs per block pair (a cluster): 1 or 2
+  unsigned split;               // CTAs per block pair (a cluster): 1, 2 or 4
+  unsigned width;               // with split 1: block pairs per CTA, 1 or 2 (l1_step2_kernel)
   unsigned steps1;              // outer steps per sweep (persistent sweep kernel)
   unsigned *ver;                // per block: CTAs that have finished writing it this sweep
 };

@@ -1125,6 +1125,21 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
   pair_step<SORT, ACCV, NSPLIT>(P, P.step, blockIdx.x / NSPLIT, rank, sm);
 }
 
+// one launch per outer step, two block pairs per CTA (a step with more pairs
+// than SMs: one wave instead of two, and the two pairs' serial phases
+// overlap): CTA c takes pairs 2c and 2c + 1 through pair_step2, or the last
+// pair alone through pair_step
+template <bool SORT, bool ACCV>
+__global__ void __launch_bounds__(kThreads, 1) l1_step2_kernel(const __grid_constant__ StepParams P)
+{
+  extern __shared__ __align__(128) double sm[];
+  const unsigned a = 2u * blockIdx.x;
+  if (a + 1u < P.pairs)
+    pair_step2<SORT, ACCV>(P, P.step, a, P, P.step, a + 1u, sm);
+  else
+    pair_step<SORT, ACCV, 1u>(P, P.step, a, 0u, sm);
+}
+
 // ---------------------------------------------------------------------------
 // One launch for a whole sweep.  Cluster c takes block pair c of every outer
 // step in turn.  A block is rewritten by exactly one pair per step, so pair
@@ -1461,10 +1476,19 @@ template <bool S, bool A, unsigned N> static cudaError_t set_smem(const int byte
   return cudaFuncSetAttribute(l1_step_kernel<S, A, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
+template <bool S, bool A> static cudaError_t set_smem2()
+{
+  return cudaFuncSetAttribute(l1_step2_kernel<S, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)batch2_smem_bytes());
+}
+
 cudaError_t l1_configure()
 {
   const int b = (int)l1_smem_bytes();
   cudaError_t e;
+  if ((e = set_smem2<false, false>()) || (e = set_smem2<false, true>()) || (e = set_smem2<true, false>()) ||
+      (e = set_smem2<true, true>()))
+    return e;
   if ((e = set_smem<false, false, 1u>(b)) || (e = set_smem<false, true, 1u>(b)) || (e = set_smem<true, false, 1u>(b)) ||
       (e = set_smem<true, true, 1u>(b)) || (e = set_smem<false, false, 2u>(b)) || (e = set_smem<false, true, 2u>(b)) ||
       (e = set_smem<true, false, 2u>(b)) || (e = set_smem<true, true, 2u>(b)) ||
@@ -1637,9 +1661,20 @@ unsigned l1_split(const unsigned pairs)
   return (4u * pairs <= (unsigned)sms) ? 4u : (2u * pairs <= (unsigned)sms) ? 2u : 1u;
 }
 
+template <bool S, bool A> static cudaError_t launch2(const StepParams &p, cudaStream_t s)
+{
+  l1_step2_kernel<S, A><<<(p.pairs + 1u) / 2u, kThreads, batch2_smem_bytes(), s>>>(p);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_l1_step(const bool sort, const bool accv, const StepParams &p, cudaStream_t s)
 {
   const unsigned n = p.split;
+  if (n == 1u && p.width == 2u) {
+    if (sort)
+      return accv ? launch2<true, true>(p, s) : launch2<true, false>(p, s);
+    return accv ? launch2<false, true>(p, s) : launch2<false, false>(p, s);
+  }
   if (n == 4u) {
     if (sort)
       return accv ? launch<true, true, 4u>(p, s) : launch<true, false, 4u>(p, s);

@@ -107,11 +107,14 @@ void gjx_set_sweep_mode(int mode);
  * for the automatic choice.  The results are the same bits for any value. */
 void gjx_set_split(unsigned n);
 
-/* Block pairs that a CTA of the batched form (gjx_hypJacL2_batched) takes
- * at a time: 2 (default; the Cholesky factorisations and inner sweeps of the
- * two run concurrently on two groups of 4 warps) or 1.  The results are the
- * same bits for either value. */
-void gjx_set_batch_width(unsigned w);
+/* Block pairs that a CTA takes at a time: 2 (the Cholesky factorisations
+ * and inner sweeps of the two run concurrently on two groups of 4 warps), 1,
+ * or 0 (default): automatic -- 2 in the batched form
+ * (gjx_hypJacL2_batched), and in the per-step launches of a single matrix
+ * with one CTA per block pair when a step has more block pairs than the GPU
+ * has SMs (one wave of CTAs instead of two); else 1.  The results are the
+ * same bits for every value. */
+void gjx_set_pairs_per_cta(unsigned w);
 
 /*
  * Autotuner: time every launch configuration of this shape -- 1, 2 or 4

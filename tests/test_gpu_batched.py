@@ -34,7 +34,7 @@ CASES = [(64, 64, 64), (128, 128, 64), (192, 192, 0), (256, 256, 256), (320, 320
 def test_batched_equals_single(built, alg, width):
     import torch
     import gpujachx_b200 as g
-    g.lib().gjx_set_batch_width(width)   # 2: two block pairs per CTA, from different matrices too
+    g.lib().gjx_set_pairs_per_cta(width)   # 2: two block pairs per CTA, from different matrices too
     g.init_strats(None, "cycwor", 32, "cycwor", 4)   # the family; each matrix takes its own n1 table
     full = bool(alg & 2)
     mats = []
@@ -45,7 +45,7 @@ def test_batched_equals_single(built, alg, width):
     batch = [_dev(G, full) for G, _ in mats]
     res = g.hypJacL2_batched(alg, [b[0] for b in batch], [p for _, p in mats], Vs=[b[1] for b in batch] if full else None,
                              Ds=[b[2] for b in batch])
-    g.lib().gjx_set_batch_width(2)
+    g.lib().gjx_set_pairs_per_cta(0)
     assert res.info == [0] * len(mats)
     for k, (G, p) in enumerate(mats):
         n = G.shape[1]

@@ -56,3 +56,30 @@ def test_cluster_sizes_give_the_same_bits(built, m, n, p, alg):
         assert (a.sweeps, a.rot_s, a.rot_b) == (b.sweeps, b.rot_s, b.rot_b)
         for x, y in ((a.U, b.U), (a.D, b.D)) + (((a.V, b.V),) if alg & 2 else ()):
             assert np.array_equal(x.view(np.uint64), y.view(np.uint64))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("m,n,p,alg,gen", [(256, 256, 256, 9, "svd_synth"), (1024, 480, 200, 11, "graded"),
+                                           (2048, 1024, 512, 3, "graded"), (640, 640, 640, 1, "gaussian"),
+                                           (512, 256, 0, 11, "gaussian")])
+def test_two_pairs_per_cta_give_the_same_bits(built, m, n, p, alg, gen):
+    """One CTA per block pair, per-step launches: two pairs per CTA (the form
+    used when a step has more pairs than SMs; 480 columns: 15 pairs per step,
+    the last one alone) against one."""
+    import gpujachx_b200 as g
+    kw = {"smin": 1e-8} if gen == "svd_synth" else {}
+    G = synth.make(gen, m, n, 79, **kw)
+    g.init_strats(None, "cycwor", 32, "cycwor", n // 16)
+    g.lib().gjx_set_split(1)
+    g.lib().gjx_set_sweep_mode(0)
+    runs = []
+    for w in (1, 2):
+        g.lib().gjx_set_pairs_per_cta(w)
+        runs.append(g.hypJacL2(alg, G, p))
+    g.lib().gjx_set_pairs_per_cta(0)
+    g.lib().gjx_set_split(0)
+    g.lib().gjx_set_sweep_mode(-1)
+    a, b = runs
+    assert (a.sweeps, a.rot_s, a.rot_b) == (b.sweeps, b.rot_s, b.rot_b)
+    for x, y in ((a.U, b.U), (a.D, b.D)) + (((a.V, b.V),) if alg & 2 else ()):
+        assert np.array_equal(x.view(np.uint64), y.view(np.uint64))
