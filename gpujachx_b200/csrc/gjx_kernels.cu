@@ -144,11 +144,87 @@ __device__ __forceinline__ void gram_tile(const double *const st, const unsigned
   }
 }
 
-// Lanes of the Gram: x-block xb (rows 4xb..4xb+3) has the lanes y = 0..4xb+3
-// (entries with y > x are computed and dropped).  A warp takes a primary
-// x-block p (lanes 0..4p+3) and possibly a secondary one s (the next 4s+4
-// lanes), so that the 4 operands of column x0+u are shared by the warp.
-//   one CTA:  warps 0..4 = (7), (6,0), (5,1), (4,2), (3)
+// The same for the 8 chains (x0+u, y0) and (x0+u, y1) of a lane (one CTA per
+// block pair): both columns share the diagonal operands, so each 16-byte
+// diagonal load feeds 4 FMAs instead of 2.
+__device__ __forceinline__ void gram_tile2(const double *const st, const unsigned base, const unsigned x0,
+                                           const unsigned y0, const unsigned y1, double (&acc)[4][2])
+{
+  const double *const yp0 = st + base + y0 * kGramColLd;
+  const double *const yp1 = st + base + y1 * kGramColLd;
+  const double *const xp = st + base + x0 * kGramColLd;
+  double2 Yb[3][2], Xb[3][4];
+#pragma unroll
+  for (unsigned q = 0u; q < 2u; ++q) {
+    const unsigned o = (x0 + 2u * q) & 63u;
+    Yb[q][0] = *reinterpret_cast<const double2 *>(yp0 + o);
+    Yb[q][1] = *reinterpret_cast<const double2 *>(yp1 + o);
+#pragma unroll
+    for (unsigned u = 0u; u < 4u; ++u)
+      Xb[q][u] = *reinterpret_cast<const double2 *>(xp + u * kGramColLd + o);
+  }
+#pragma unroll
+  for (unsigned kp = 0u; kp < 34u; ++kp) { // pairs k = 2kp, 2kp + 1
+    if (kp + 2u < 34u) {
+      const unsigned q = (kp + 2u) % 3u;
+      const unsigned o = (x0 + 2u * (kp + 2u)) & 63u;
+      Yb[q][0] = *reinterpret_cast<const double2 *>(yp0 + o);
+      Yb[q][1] = *reinterpret_cast<const double2 *>(yp1 + o);
+#pragma unroll
+      for (unsigned u = 0u; u < 4u; ++u)
+        if (2u * (kp + 2u) + 1u >= u && 2u * (kp + 2u) <= u + 63u)
+          Xb[q][u] = *reinterpret_cast<const double2 *>(xp + u * kGramColLd + o);
+    }
+    const unsigned q = kp % 3u;
+#pragma unroll
+    for (unsigned h = 0u; h < 2u; ++h) {
+      const unsigned k = 2u * kp + h;
+#pragma unroll
+      for (unsigned v = 0u; v < 2u; ++v) {
+        const double yv = h ? Yb[q][v].y : Yb[q][v].x;
+#pragma unroll
+        for (unsigned u = 0u; u < 4u; ++u)
+          if (k >= u && k <= u + 63u)
+            acc[u][v] = __fma_rn(yv, h ? Xb[q][u].y : Xb[q][u].x, acc[u][v]);
+      }
+    }
+  }
+}
+
+// Lanes of gram_tile2 (one CTA per pair): x-block b (rows 4b..4b+3) has
+// 2(b+1) lanes; its lane j takes columns y0 = j and y1 = j + 2(b+1), i.e. all
+// y = 0..4b+3 (entries with y > x are computed and dropped).  72 lanes in 3
+// warps: x-blocks (7, 6, 0), (5, 4, 3), (2, 1).
+__device__ __forceinline__ bool gram_lane2(const unsigned warp, const unsigned lane, unsigned &x0, unsigned &y0,
+                                           unsigned &y1)
+{
+  if (warp >= 3u)
+    return false;
+  unsigned first = 0u;
+#pragma unroll
+  for (unsigned i = 0u; i < 3u; ++i) {
+    const int b = (warp == 0u) ? ((i == 0u) ? 7 : (i == 1u) ? 6 : 0)
+                               : (warp == 1u) ? ((i == 0u) ? 5 : (i == 1u) ? 4 : 3) : ((i == 0u) ? 2 : (i == 1u) ? 1 : -1);
+    if (b < 0)
+      return false;
+    const unsigned nl = 2u * (unsigned)b + 2u;
+    if (lane < first + nl) {
+      const unsigned j = lane - first;
+      x0 = 4u * (unsigned)b;
+      y0 = j;
+      y1 = j + nl;
+      return true;
+    }
+    first += nl;
+  }
+  return false;
+}
+
+// Lanes of gram_tile (2- and 4-CTA clusters): x-block xb (rows 4xb..4xb+3)
+// has the lanes y = 0..4xb+3 (entries with y > x are computed and dropped).
+// A warp takes a primary x-block p (lanes 0..4p+3) and possibly a secondary
+// one s (the next 4s+4 lanes), so that the 4 operands of column x0+u are
+// shared by the warp.
 //   2-CTA cluster, rank 0: (7), (6,0), (1); rank 1: (5), (4,2), (3)
 //   4-CTA cluster, rank r: (7 - r), (r)
 template <unsigned NSPLIT>
@@ -162,12 +238,7 @@ __device__ __forceinline__ bool gram_lane_of(const unsigned rank, const unsigned
     p = (warp == 0u) ? 7 - (int)rank : (int)rank;
     sb = -1;
   }
-  else if (NSPLIT == 1u) { // (7), (6,0), (5,1), (4,2), (3)
-    if (warp >= 5u)
-      return false;
-    p = 7 - (int)warp;
-    sb = (warp >= 1u && warp <= 3u) ? (int)warp - 1 : -1;
-  } else { // rank 0: (7), (6,0), (1); rank 1: (5), (4,2), (3)
+  else { // rank 0: (7), (6,0), (1); rank 1: (5), (4,2), (3)
     if (warp >= 3u)
       return false;
     p = (rank == 0u) ? ((warp == 2u) ? 1 : 7 - (int)warp) : 5 - (int)warp;
@@ -708,10 +779,16 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
 
   // ------------------------------ 1. Gram --------------------------------
   const unsigned ntile = P.nrow >> 6; // 64-row tiles
-  unsigned gx0 = 0u, gy = 0u;
-  const unsigned gwarps = (NSPLIT == 4u) ? 2u : (NSPLIT == 2u) ? 3u : 5u;
-  const bool gthr = gram_lane_of<NSPLIT>(rank, warp, lane, gx0, gy);
+  // one CTA per pair: 8 chains per lane (gram_tile2, 3 warps); else 4 (gram_tile)
+  unsigned gx0 = 0u, gy = 0u, gy1 = 0u;
+  const unsigned gwarps = (NSPLIT == 4u) ? 2u : 3u;
+  bool gthr;
+  if constexpr (NSPLIT == 1u)
+    gthr = gram_lane2(warp, lane, gx0, gy, gy1);
+  else
+    gthr = gram_lane_of<NSPLIT>(rank, warp, lane, gx0, gy);
   double gacc[4] = {+0.0, +0.0, +0.0, +0.0};
+  double gacc2[4][2] = {{+0.0, +0.0}, {+0.0, +0.0}, {+0.0, +0.0}, {+0.0, +0.0}};
 
   const unsigned ngst = (ntile + kGramTiles - 1u) / kGramTiles; // stages of 2 tiles
   // thread 0: the TMA engine brings stage k, per tile block i's and block j's
@@ -742,8 +819,12 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
         fail = 1;
       else if (gthr) {
         const unsigned nt = min(kGramTiles, ntile - k * kGramTiles);
-        for (unsigned t = 0u; t < nt; ++t)
-          gram_tile(stg + (k % kGramStages) * kGramStage, t * kGramTileLd, gx0, gy, gacc);
+        for (unsigned t = 0u; t < nt; ++t) {
+          if constexpr (NSPLIT == 1u)
+            gram_tile2(stg + (k % kGramStages) * kGramStage, t * kGramTileLd, gx0, gy, gy1, gacc2);
+          else
+            gram_tile(stg + (k % kGramStages) * kGramStage, t * kGramTileLd, gx0, gy, gacc);
+        }
       }
     }
     failed = __syncthreads_or(fail); // uniform decision
@@ -756,7 +837,19 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
     atomicOr(P.err, kErrWaitTimeout);
   }
   // our share of the lower triangle, into our R and the other CTAs' R
-  if (gthr) {
+  if constexpr (NSPLIT == 1u) {
+    if (gthr) {
+#pragma unroll
+      for (unsigned u = 0u; u < 4u; ++u)
+#pragma unroll
+        for (unsigned v = 0u; v < 2u; ++v) {
+          const unsigned y = v ? gy1 : gy;
+          if (gx0 + u >= y)
+            R[y * 32u + gx0 + u] = gacc2[u][v];
+        }
+    }
+  }
+  else if (gthr) {
 #pragma unroll
     for (unsigned u = 0u; u < 4u; ++u)
       if (gx0 + u >= gy) {
@@ -919,9 +1012,9 @@ __device__ __forceinline__ void pair_step2(const StepParams &PA, const unsigned 
   const unsigned ntA = PA.nrow >> 6, ntB = PB.nrow >> 6;
   const unsigned ngA = (ntA + kGramTiles - 1u) / kGramTiles, ngB = (ntB + kGramTiles - 1u) / kGramTiles;
   const unsigned ng = ngA + ngB;
-  unsigned gx0 = 0u, gy = 0u;
-  const bool gthr = gram_lane_of<1u>(0u, warp, lane, gx0, gy);
-  double gacc[4] = {+0.0, +0.0, +0.0, +0.0};
+  unsigned gx0 = 0u, gy = 0u, gy1 = 0u;
+  const bool gthr = gram_lane2(warp, lane, gx0, gy, gy1);
+  double gacc[4][2] = {{+0.0, +0.0}, {+0.0, +0.0}, {+0.0, +0.0}, {+0.0, +0.0}};
   auto stage_tiles = [&](const unsigned k) {
     return (k < ngA) ? min(kGramTiles, ntA - k * kGramTiles) : min(kGramTiles, ntB - (k - ngA) * kGramTiles);
   };
@@ -941,11 +1034,14 @@ __device__ __forceinline__ void pair_step2(const StepParams &PA, const unsigned 
   auto put_gram = [&](double *const R) { // our share of the lower triangle
     if (gthr) {
 #pragma unroll
-      for (unsigned u = 0u; u < 4u; ++u) {
-        if (gx0 + u >= gy)
-          R[gy * 32u + gx0 + u] = gacc[u];
-        gacc[u] = +0.0;
-      }
+      for (unsigned u = 0u; u < 4u; ++u)
+#pragma unroll
+        for (unsigned v = 0u; v < 2u; ++v) {
+          const unsigned y = v ? gy1 : gy;
+          if (gx0 + u >= y)
+            R[y * 32u + gx0 + u] = gacc[u][v];
+          gacc[u][v] = +0.0;
+        }
     }
   };
 
@@ -958,13 +1054,13 @@ __device__ __forceinline__ void pair_step2(const StepParams &PA, const unsigned 
     if (tid == kIssuer && k + kGramStages - 1u < ng)
       issue_gram(k + kGramStages - 1u);
     int fail = 0;
-    if (warp < 5u) {
+    if (warp < 3u) {
       if (!mbar_wait_bounded(&bars[k % kGramStages], (k / kGramStages) & 1u, kWaitLimit))
         fail = 1;
       else if (gthr) {
         const unsigned nt = stage_tiles(k);
         for (unsigned t = 0u; t < nt; ++t)
-          gram_tile(stg + (k % kGramStages) * kGramStage, t * kGramTileLd, gx0, gy, gacc);
+          gram_tile2(stg + (k % kGramStages) * kGramStage, t * kGramTileLd, gx0, gy, gy1, gacc);
       }
       if (k + 1u == ngA)
         put_gram(sm + kOffR);
