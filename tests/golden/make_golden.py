@@ -131,7 +131,8 @@ def main():
     if "--variant" in sys.argv:
         variant = sys.argv[sys.argv.index("--variant") + 1]
         args = [a for a in args if a != variant]
-    out_path = args[0] if args else os.path.join(ROOT, "gpurun_out", f"ref_golden_{variant}.json")
+    out_path = args[0] if args else os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                                                f"ref_golden_{variant}.json")
     res = []
     for c in CASES:
         G = make_input(c)
