@@ -220,30 +220,88 @@ __device__ __forceinline__ bool gram_lane2(const unsigned warp, const unsigned l
   return false;
 }
 
-// Lanes of gram_tile (2- and 4-CTA clusters): x-block xb (rows 4xb..4xb+3)
+// The 2 chains (x0, y) and (x0+1, y) of a lane, in acc[0] and acc[1]
+// (4-CTA clusters: each CTA has a quarter of the entries, and thinner lane
+// tiles give it 3 warps): chain u takes the k in [u, u+63], so 33 row pairs.
+__device__ __forceinline__ void gram_tile_n2(const double *const st, const unsigned base, const unsigned x0,
+                                             const unsigned y, double (&acc)[4])
+{
+  const double *const yp = st + base + y * kGramColLd;
+  const double *const xp = st + base + x0 * kGramColLd;
+  double2 Yb[3], Xb[3][2];
+#pragma unroll
+  for (unsigned q = 0u; q < 2u; ++q) {
+    const unsigned o = (x0 + 2u * q) & 63u;
+    Yb[q] = *reinterpret_cast<const double2 *>(yp + o);
+#pragma unroll
+    for (unsigned u = 0u; u < 2u; ++u)
+      Xb[q][u] = *reinterpret_cast<const double2 *>(xp + u * kGramColLd + o);
+  }
+#pragma unroll
+  for (unsigned kp = 0u; kp < 33u; ++kp) { // pairs k = 2kp, 2kp + 1
+    if (kp + 2u < 33u) {
+      const unsigned q = (kp + 2u) % 3u;
+      const unsigned o = (x0 + 2u * (kp + 2u)) & 63u;
+      Yb[q] = *reinterpret_cast<const double2 *>(yp + o);
+#pragma unroll
+      for (unsigned u = 0u; u < 2u; ++u)
+        if (2u * (kp + 2u) + 1u >= u && 2u * (kp + 2u) <= u + 63u)
+          Xb[q][u] = *reinterpret_cast<const double2 *>(xp + u * kGramColLd + o);
+    }
+    const unsigned q = kp % 3u;
+#pragma unroll
+    for (unsigned h = 0u; h < 2u; ++h) {
+      const unsigned k = 2u * kp + h;
+      const double yv = h ? Yb[q].y : Yb[q].x;
+#pragma unroll
+      for (unsigned u = 0u; u < 2u; ++u)
+        if (k >= u && k <= u + 63u)
+          acc[u] = __fma_rn(yv, h ? Xb[q][u].y : Xb[q][u].x, acc[u]);
+    }
+  }
+}
+
+// Lanes of gram_tile_n2 in a 4-CTA cluster: x-block b (rows 2b, 2b+1) has the
+// lanes y = 0..2b+1 (entries with y > x are computed and dropped); CTA r
+// takes x-blocks 15-r (warp 0), 8+r then r (warp 1) and 7-r (warp 2): 68
+// lanes in every CTA.
+__device__ __forceinline__ bool gram_lane_q(const unsigned rank, const unsigned warp, const unsigned lane,
+                                            unsigned &x0, unsigned &y)
+{
+  unsigned b, first = 0u;
+  if (warp == 0u)
+    b = 15u - rank;
+  else if (warp == 1u) {
+    const unsigned n1 = 2u * (8u + rank) + 2u;
+    b = (lane < n1) ? 8u + rank : rank;
+    first = (lane < n1) ? 0u : n1;
+  }
+  else if (warp == 2u)
+    b = 7u - rank;
+  else
+    return false;
+  if (lane >= first + 2u * b + 2u)
+    return false;
+  x0 = 2u * b;
+  y = lane - first;
+  return true;
+}
+
+// Lanes of gram_tile (2-CTA clusters): x-block xb (rows 4xb..4xb+3)
 // has the lanes y = 0..4xb+3 (entries with y > x are computed and dropped).
 // A warp takes a primary x-block p (lanes 0..4p+3) and possibly a secondary
 // one s (the next 4s+4 lanes), so that the 4 operands of column x0+u are
 // shared by the warp.
-//   2-CTA cluster, rank 0: (7), (6,0), (1); rank 1: (5), (4,2), (3)
-//   4-CTA cluster, rank r: (7 - r), (r)
+//   rank 0: (7), (6,0), (1); rank 1: (5), (4,2), (3)
 template <unsigned NSPLIT>
 __device__ __forceinline__ bool gram_lane_of(const unsigned rank, const unsigned warp, const unsigned lane,
                                              unsigned &x0, unsigned &y)
 {
-  int p, sb;
-  if (NSPLIT == 4u) { // rank r: warps (7 - r), (r)
-    if (warp >= 2u)
-      return false;
-    p = (warp == 0u) ? 7 - (int)rank : (int)rank;
-    sb = -1;
-  }
-  else { // rank 0: (7), (6,0), (1); rank 1: (5), (4,2), (3)
-    if (warp >= 3u)
-      return false;
-    p = (rank == 0u) ? ((warp == 2u) ? 1 : 7 - (int)warp) : 5 - (int)warp;
-    sb = (warp == 1u) ? (rank == 0u ? 0 : 2) : -1;
-  }
+  static_assert(NSPLIT == 2u, "the lane map of 2-CTA clusters");
+  if (warp >= 3u) // rank 0: (7), (6,0), (1); rank 1: (5), (4,2), (3)
+    return false;
+  const int p = (rank == 0u) ? ((warp == 2u) ? 1 : 7 - (int)warp) : 5 - (int)warp;
+  const int sb = (warp == 1u) ? (rank == 0u ? 0 : 2) : -1;
   const unsigned np = 4u * (unsigned)p + 4u;
   if (lane < np) {
     x0 = 4u * (unsigned)p;
@@ -779,12 +837,15 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
 
   // ------------------------------ 1. Gram --------------------------------
   const unsigned ntile = P.nrow >> 6; // 64-row tiles
-  // one CTA per pair: 8 chains per lane (gram_tile2, 3 warps); else 4 (gram_tile)
+  // chains per lane: 8 with one CTA per pair (gram_tile2), 4 with 2 CTAs
+  // (gram_tile), 2 with 4 CTAs (gram_tile_n2); 3 Gram warps each
   unsigned gx0 = 0u, gy = 0u, gy1 = 0u;
-  const unsigned gwarps = (NSPLIT == 4u) ? 2u : 3u;
+  const unsigned gwarps = 3u;
   bool gthr;
   if constexpr (NSPLIT == 1u)
     gthr = gram_lane2(warp, lane, gx0, gy, gy1);
+  else if constexpr (NSPLIT == 4u)
+    gthr = gram_lane_q(rank, warp, lane, gx0, gy);
   else
     gthr = gram_lane_of<NSPLIT>(rank, warp, lane, gx0, gy);
   double gacc[4] = {+0.0, +0.0, +0.0, +0.0};
@@ -822,6 +883,8 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
         for (unsigned t = 0u; t < nt; ++t) {
           if constexpr (NSPLIT == 1u)
             gram_tile2(stg + (k % kGramStages) * kGramStage, t * kGramTileLd, gx0, gy, gy1, gacc2);
+          else if constexpr (NSPLIT == 4u)
+            gram_tile_n2(stg + (k % kGramStages) * kGramStage, t * kGramTileLd, gx0, gy, gacc);
           else
             gram_tile(stg + (k % kGramStages) * kGramStage, t * kGramTileLd, gx0, gy, gacc);
         }
@@ -851,7 +914,7 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
   }
   else if (gthr) {
 #pragma unroll
-    for (unsigned u = 0u; u < 4u; ++u)
+    for (unsigned u = 0u; u < ((NSPLIT == 4u) ? 2u : 4u); ++u)
       if (gx0 + u >= gy) {
         const unsigned o = gy * 32u + gx0 + u;
         R[o] = gacc[u];
