@@ -305,6 +305,9 @@ __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.comm
 // this thread's bulk groups have finished reading shared memory
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 
+// all but this thread's most recent bulk group have finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read_but1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+
 // this thread's bulk groups are complete (their global writes performed),
 // and ordered before this thread's later generic-proxy operations
 __device__ __forceinline__ void bulk_wait_all()

@@ -95,6 +95,19 @@ constexpr unsigned kSmemDoubles = kOffBar + 8u;
 
 size_t l1_smem_bytes() { return (size_t)kSmemDoubles * sizeof(double); }
 
+// the step kernels of 2- and 4-CTA clusters keep a third update buffer after
+// the rest (128-byte aligned), 227 KB in all
+constexpr unsigned kOffUpd3 = (kSmemDoubles + 15u) & ~15u;
+constexpr unsigned kSmemDoubles3 = kOffUpd3 + kUpdStage;
+static_assert(kSmemDoubles3 * sizeof(double) <= 227u * 1024u, "the third update buffer must fit");
+template <unsigned NSPLIT> struct UpdBuffers {
+  static constexpr unsigned value = (NSPLIT > 1u) ? 3u : 2u;
+};
+size_t step_smem_bytes(const unsigned nsplit)
+{
+  return (size_t)((nsplit > 1u) ? kSmemDoubles3 : kSmemDoubles) * sizeof(double);
+}
+
 #define E32(A, r, c) (A)[(c) * 32u + (r)]
 
 // ---------------------------------------------------------------------------
@@ -811,10 +824,13 @@ __device__ __forceinline__ void add_counts(const StepParams &P, const unsigned b
 // ---------------------------------------------------------------------------
 // The block-pair step kernel.
 // ---------------------------------------------------------------------------
-template <bool SORT, bool ACCV, unsigned NSPLIT>
+// NBUF update buffers: 2 in the region of the Gram stages, a third (NBUF = 3)
+// at kOffUpd3 where the launch provides it
+template <bool SORT, bool ACCV, unsigned NSPLIT, unsigned NBUF = 2u>
 __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned step, const unsigned pair,
                                           const unsigned rank, double *const sm)
 {
+  static_assert(NBUF == 2u || NBUF == 3u, "2 or 3 update buffers");
   double *const stg = sm;
   double *const R = sm + kOffR;
   double *const Vl = sm + kOffVl;
@@ -939,12 +955,13 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
   const unsigned nV = ACCV ? (P.ncol + kUpdRows - 1u) / kUpdRows : 0u;
   const unsigned nst = nG + nV;
   const unsigned nmine = (nst > rank) ? (nst - rank + NSPLIT - 1u) / NSPLIT : 0u;
+  auto ubuf = [&](const unsigned s) { return (NBUF == 3u && s == 2u) ? sm + kOffUpd3 : stg + s * kUpdStage; };
   auto issue_upd = [&](const unsigned i) { // one thread: this CTA's i-th stage, 2 tensor copies
-    const unsigned k = rank + i * NSPLIT, s = i % kUpdStages;
+    const unsigned k = rank + i * NSPLIT, s = i % NBUF;
     const bool isG = k < nG;
     const CUtensorMap *const tm = isG ? &P.tmG : &P.tmV;
     const int piece = (int)(((isG ? k : (k - nG)) * kUpdRows) >> 5);
-    double *const st = stg + s * kUpdStage;
+    double *const st = ubuf(s);
     mbar_arrive_expect_tx(&bars[4u + s], 2u * kUpdBoxBytes);
     tma_load_3d(st, tm, 0, piece, (int)(iBlk * kNColB), &bars[4u + s]);
     tma_load_3d(st + 16u * kUpdColLd, tm, 0, piece, (int)(jBlk * kNColB), &bars[4u + s]);
@@ -981,20 +998,25 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
   }
 
   __syncthreads(); // VT ready
-  // stage i: thread 0 issues the copy of stage i + 1 into the other buffer
-  // once the store of stage i - 1 has read it out; the warps compute stage i
-  // and put the results in place; after the barrier thread 0 stores them
-  // with two tensor copies, which overlap the next stage's arithmetic
+  // stage i: thread 0 issues the copy of stage i + 1 into its buffer once the
+  // store that last used that buffer has read it out (with 2 buffers the
+  // store of stage i - 1, issued just before; with 3 that of stage i - 2, a
+  // stage ago); the warps compute stage i and put the results in place;
+  // after the barrier thread 0 stores them with two tensor copies, which
+  // overlap the next stage's arithmetic
   const unsigned rg = warp, sub = lane & 7u, cg8 = lane >> 3;
   for (unsigned i = 0u; i < nmine; ++i) {
     if (tid == 0u && i + 1u < nmine) {
-      bulk_wait_read();
+      if (NBUF == 3u)
+        bulk_wait_read_but1();
+      else
+        bulk_wait_read();
       issue_upd(i + 1u);
     }
     // a warp computes only if all its lanes saw the stage land
-    const int fail = !__all_sync(0xffffffffu, mbar_wait_bounded(&bars[4u + (i % kUpdStages)], (i / kUpdStages) & 1u,
+    const int fail = !__all_sync(0xffffffffu, mbar_wait_bounded(&bars[4u + (i % NBUF)], (i / NBUF) & 1u,
                                                                 kWaitLimit));
-    double *const sb = stg + (i % kUpdStages) * kUpdStage;
+    double *const sb = ubuf(i % NBUF);
     if (!fail) {
       double acc[4][8]; // the whole warp computes (rows past the end: not stored)
       update_stage(sb, VT, rg, sub, cg8, acc);
@@ -1004,10 +1026,9 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
     }
     if (__syncthreads_or(fail)) { // uniform decision; drain (bounded), report
       if (tid == 0u) {
-        (void)mbar_wait_bounded(&bars[4u + (i % kUpdStages)], (i / kUpdStages) & 1u, kWaitLimit / 8);
+        (void)mbar_wait_bounded(&bars[4u + (i % NBUF)], (i / NBUF) & 1u, kWaitLimit / 8);
         if (i + 1u < nmine)
-          (void)mbar_wait_bounded(&bars[4u + ((i + 1u) % kUpdStages)], ((i + 1u) / kUpdStages) & 1u,
-                                  kWaitLimit / 8);
+          (void)mbar_wait_bounded(&bars[4u + ((i + 1u) % NBUF)], ((i + 1u) / NBUF) & 1u, kWaitLimit / 8);
         bulk_wait_all();
         atomicOr(P.err, kErrWaitTimeout);
       }
@@ -1281,7 +1302,7 @@ __global__ void __launch_bounds__(kThreads, 1) l1_step_kernel(const __grid_const
 {
   extern __shared__ __align__(128) double sm[];
   const unsigned rank = (NSPLIT > 1u) ? (blockIdx.x % NSPLIT) : 0u;
-  pair_step<SORT, ACCV, NSPLIT>(P, P.step, blockIdx.x / NSPLIT, rank, sm);
+  pair_step<SORT, ACCV, NSPLIT, UpdBuffers<NSPLIT>::value>(P, P.step, blockIdx.x / NSPLIT, rank, sm);
 }
 
 // one launch per outer step, two block pairs per CTA (a step with more pairs
@@ -1356,7 +1377,7 @@ __global__ void __launch_bounds__(kThreads, 1) l1_sweep_kernel(const __grid_cons
     if (!all)
       break; // the same decision in every CTA of the cluster
     asm volatile("fence.proxy.async;" ::: "memory"); // the copies below read what other SMs wrote
-    pair_step<SORT, ACCV, NSPLIT>(P, step, pair, rank, sm);
+    pair_step<SORT, ACCV, NSPLIT, UpdBuffers<NSPLIT>::value>(P, step, pair, rank, sm);
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0u) {
@@ -1648,11 +1669,12 @@ cudaError_t l1_configure()
   if ((e = set_smem2<false, false>()) || (e = set_smem2<false, true>()) || (e = set_smem2<true, false>()) ||
       (e = set_smem2<true, true>()))
     return e;
+  const int b3 = (int)step_smem_bytes(2u);
   if ((e = set_smem<false, false, 1u>(b)) || (e = set_smem<false, true, 1u>(b)) || (e = set_smem<true, false, 1u>(b)) ||
-      (e = set_smem<true, true, 1u>(b)) || (e = set_smem<false, false, 2u>(b)) || (e = set_smem<false, true, 2u>(b)) ||
-      (e = set_smem<true, false, 2u>(b)) || (e = set_smem<true, true, 2u>(b)) ||
-      (e = set_smem<false, false, 4u>(b)) || (e = set_smem<false, true, 4u>(b)) ||
-      (e = set_smem<true, false, 4u>(b)) || (e = set_smem<true, true, 4u>(b)))
+      (e = set_smem<true, true, 1u>(b)) || (e = set_smem<false, false, 2u>(b3)) || (e = set_smem<false, true, 2u>(b3)) ||
+      (e = set_smem<true, false, 2u>(b3)) || (e = set_smem<true, true, 2u>(b3)) ||
+      (e = set_smem<false, false, 4u>(b3)) || (e = set_smem<false, true, 4u>(b3)) ||
+      (e = set_smem<true, false, 4u>(b3)) || (e = set_smem<true, true, 4u>(b3)))
     return e;
   return cudaSuccess;
 }
@@ -1662,7 +1684,7 @@ template <bool S, bool A, unsigned N> static cudaError_t launch(const StepParams
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(p.pairs * N);
   cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes = l1_smem_bytes();
+  cfg.dynamicSmemBytes = step_smem_bytes(N);
   cfg.stream = s;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -1742,7 +1764,7 @@ template <bool S, bool A, unsigned N> static cudaLaunchConfig_t sweep_cfg(const 
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(p.pairs * N);
   cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes = l1_smem_bytes();
+  cfg.dynamicSmemBytes = step_smem_bytes(N);
   cfg.stream = s;
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = N;
@@ -1758,7 +1780,7 @@ template <bool S, bool A, unsigned N> static cudaLaunchConfig_t sweep_cfg(const 
 template <bool S, bool A, unsigned N> static bool sweep_fits(const StepParams &p)
 {
   if (cudaFuncSetAttribute(l1_sweep_kernel<S, A, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)l1_smem_bytes()) != cudaSuccess)
+                           (int)step_smem_bytes(N)) != cudaSuccess)
     return false;
   cudaLaunchAttribute at[2];
   cudaLaunchConfig_t cfg = sweep_cfg<S, A, N>(p, nullptr, at);
