@@ -84,7 +84,7 @@ cudaError_t launch_batch_initD(const BatchMat *m, unsigned nmat, const uint32_t 
 
 // TMA tensor maps for the update staging (3-D view, box {34, 8, 16}); 0 or a CUDA error
 cudaError_t make_update_map(CUtensorMap *tm, const double *base, unsigned nrow, unsigned ncol, unsigned ld);
-// TMA tensor map for the Gram staging (4-D view, box {34, 3, 1, 16})
+// TMA tensor map for the Gram staging (3-D view, box {66, 1, 16})
 cudaError_t make_gram_map(CUtensorMap *tm, const double *base, unsigned nrow, unsigned ncol, unsigned ld);
 
 // device error codes written to *err

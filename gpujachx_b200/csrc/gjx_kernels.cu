@@ -10,11 +10,13 @@
 //      bank-skewed, zero-padded layout, mbarrier completion, 4 stages of 2
 //      tiles) and computes its share of the 528 entries; every
 //      entry is one FMA chain in the reference's row order
-//      (share/device_code_common_Cholesky.hpp:4-56).  A lane holds the 4
-//      chains (x0..x0+3, y) of one column y: the operands of column x0+u are
-//      shared by the warp, column y slides through a 4-row window, and all
-//      operands come as 16-byte row pairs.  The shares are exchanged through
-//      distributed shared memory, then one cluster barrier.
+//      (share/device_code_common_Cholesky.hpp:4-56).  A lane holds the
+//      chains (x0..x0+3, y) of one column y (2-CTA clusters), also of a
+//      second column (one CTA per pair), or (x0, x0+1; y) (4-CTA clusters):
+//      the operands of the x columns are shared by the warp, the y columns
+//      slide through a row window, and all operands come as 16-byte row
+//      pairs.  The shares are exchanged through distributed shared memory,
+//      then one cluster barrier.
 //   2. 32x32 Cholesky by the CTA with a one-column look-ahead: warp 0 updates
 //      and pivots the next column while warps 1-7 update the rest
 //      (share/device_code_common_Cholesky.hpp:58-158).
@@ -33,6 +35,10 @@
 //      (share/device_code_common.hpp:146-185), computed in 4x8 register
 //      tiles along anti-diagonals, put back in place of the stage's operands
 //      and written out by TMA tensor stores that overlap the next stage.
+//
+// pair_step2 runs two block pairs in one CTA (the batched form, and steps
+// with more pairs than SMs): steps 1 and 4 of the two one after the other on
+// all warps, steps 2 and 3 concurrently on two groups of 4 warps.
 //
 // All arithmetic is in the reference's order, so results are bit-identical.
 #include <cooperative_groups.h>
