@@ -21,9 +21,11 @@ decomposition to convergence.  Metric: matrices per second (whole job).
 N > 1: independent replicas (the single-matrix SVD is not sharded), barrier
 and max-over-ranks device time; value = matrices of all ranks / that time.
 
---impl reference: the reference path timed on the host cores -- the CPU
-oracle port of the reference arithmetic (the reference itself is GPU code
-only) -- plus, when present, the reference's own GPU build timed once.
+--impl reference: the reference's own implementation of the path -- its
+hypJacL2 sources built for sm_100a (oracle/_ref/ref_harness; the reference
+is GPU code only) -- on the same input, whole decompositions timed by its own
+timer (value: its compute phase; e2e: its wall time with its own allocation
+and copies); the CPU oracle port of its arithmetic is reported beside it.
 """
 
 from __future__ import annotations
@@ -93,19 +95,6 @@ def _use(name: str) -> None:
 
 def _input() -> np.ndarray:
     from gpujachx_b200 import synth
-    if WL["gen"] == "haar_gpu":          # too large for a CPU QR at bench start-up
-        import torch
-        dev = torch.device("cuda", torch.cuda.current_device())
-        gen = torch.Generator(device=dev)
-        gen.manual_seed(SEED)
-
-        def haar(n):
-            q, r = torch.linalg.qr(torch.randn((n, n), dtype=torch.float64, device=dev, generator=gen))
-            return q * torch.sign(torch.diagonal(r)).unsqueeze(0)
-
-        sv = torch.logspace(0.0, float(np.log10(WL["kw"]["smin"])), N, dtype=torch.float64, device=dev)
-        G = (haar(M)[:, :N] * sv) @ haar(N).T
-        return np.asfortranarray(G.cpu().numpy())
     return synth.make(WL["gen"], M, N, SEED, **WL["kw"])
 
 
@@ -121,18 +110,10 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-PROFILE = os.path.join(ROOT, "profiles", "l1_step_kernel_svd4096x2048.md")
-
-
-def _profiled_traffic():
-    """DRAM bytes (read + write) of one block-pair launch of this workload, as
-    recorded from an ncu capture of it; None when no capture is recorded."""
-    import re
-    if not os.path.exists(PROFILE):
-        return None
-    with open(PROFILE) as f:
-        m = re.search(r"traffic per launch \(read \+ write\) \| ([0-9.]+) MB", f.read())
-    return float(m.group(1)) * 1e6 if m else None
+# DRAM bytes (read + write) of one block-pair launch of the c2 workload, from
+# one ncu capture of it (cold L2): dram__bytes_read.sum + dram__bytes_write.sum
+# of gjx::l1_step_kernel<true,true,2>, 4096 x 2048, ALG 11
+RECORDED_TRAFFIC = {"c2": 144.64e6}
 
 
 class Clocks:
@@ -211,7 +192,8 @@ def cpu_port_sample(G0: np.ndarray, sweeps: int, min_seconds: float = 10.0):
     per_matrix = dt / done * STEPS1 * sweeps
     return {"value": 1.0 / per_matrix, "unit": "matrices/s", "cores": cores, "kind": "port",
             "sample": f"first {done} of {STEPS1} outer steps of sweep 1 ({done * PAIRS} block pairs, "
-                      f"{dt:.1f} s), scaled x{STEPS1}/{done} steps x {sweeps} sweeps"}
+                      f"{dt:.1f} s), scaled x{STEPS1}/{done} steps x {sweeps} sweeps",
+            "seconds": dt, "outer_steps": done}
 
 
 def lapack_baseline(G0: np.ndarray):
@@ -260,76 +242,110 @@ def accuracy_figures(G0: np.ndarray, U: np.ndarray, V, D: np.ndarray) -> dict:
     return out
 
 
-def ref_gpu_once(G0: np.ndarray):
-    """The reference's own hypJacL2 built for sm_100a (oracle/_ref), one run."""
+REF_BUILD = "reference sources (1/, share/), nvcc -arch sm_100a -DUSE_RSQRT -O3, oracle/_ref/ref_harness"
+
+
+def ref_gpu_runs(G0: np.ndarray, m, n, nplus, alg, steps: int, warmup: int, budget_s: float = 240.0):
+    """The reference's own hypJacL2 built for sm_100a (oracle/_ref/ref_harness)
+    on G0: one probe run, then warmup + timed runs in one process, as many
+    timed runs as `steps` asks for while they fit in budget_s.  Returns None
+    when the reference build is absent."""
     from tests.golden.make_golden import HARNESS, case, run_ref
     if not os.path.exists(HARNESS["base"]):
         return None
-    c = case("bench", M, N, NPLUS, ALG, seed=SEED)
-    out = run_ref(c, G0)
-    t = out["timing"]
-    return {"s_per_matrix_wall": t[0], "s_per_matrix_compute": t[2], "sweeps": out["sweeps"],
-            "matrices_per_s_wall": 1.0 / t[0], "build": "reference sources, nvcc -arch sm_100a -DUSE_RSQRT -O3"}
+    c = case("bench", m, n, nplus, alg, seed=SEED)
+    probe = run_ref(c, G0)
+    t1 = max(probe["timing"][0], 1e-3)
+    timed = max(1, min(steps, int(budget_s / t1)))
+    warm = min(warmup, max(0, int(0.25 * budget_s / t1)))
+    out = run_ref(c, G0, reps=warm + timed, timeout=max(600, int(4 * t1 * (warm + timed))))
+    runs = out["reps_timing"][warm:]
+    return {"wall_s": [r[0] for r in runs], "compute_s": [r[2] for r in runs], "sweeps": out["sweeps"],
+            "rot_s": out["rot_s"], "rot_b": out["rot_b"], "warmup": warm, "steps": len(runs), "build": REF_BUILD}
 
 
 def reference_arm_batch(args):
-    """c5 on the reference path: per n, one decomposition by the CPU oracle
-    port (all host threads) and one by the reference's own sm_100a build,
-    each scaled by how many matrices of that n the batch holds."""
-    from oracle import oracle as O
+    """c5 on the reference path: the reference's own sm_100a build has no
+    batched form, so it is looped -- per batch size n, one SVD (NPLUS = n)
+    and one HSVD (NPLUS = n/2) matrix of that n, each timed over repeated runs
+    in one process (its compute phase and wall time), scaled by how many
+    matrices of that n the batch holds.  The CPU oracle port, one
+    decomposition of each, is reported beside it (cpu_baseline)."""
     from gpujachx_b200 import STRAT_PATH, synth
+    from tests.golden.make_golden import HARNESS, case, run_ref
     cfg = WORKLOADS["c5"]
     sizes = batch_sizes(cfg["count"], cfg["seed"])
-    O.build()
-    cores = os.cpu_count() or 1
-    s0 = O.load_strat(STRAT_PATH, "cycwor", 32)
-    vals, ref_by, cpu_by = [], {}, {}
-    for _ in range(max(1, args.steps)):
-        tot = 0.0
-        for n in sorted(set(int(x) for x in sizes)):
+    ns = sorted(set(int(x) for x in sizes))
+    base = {"metric": cfg["metric"], "unit": "matrices/s", "impl": "reference", "n_gpus": args.gpus,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": cfg["workload"], "name": "c5", "count": len(sizes), "alg": ALG,
+                       "parallelism": "independent batches per rank" if args.gpus > 1 else "single GPU"}}
+    line = None
+    if os.path.exists(HARNESS["base"]):
+        comp_tot = wall_tot = 0.0
+        by_n = {}
+        reps = max(1, min(args.steps, 5))
+        for n in ns:
             cnt = int((sizes == n).sum())
+            G = synth.make("svd_synth", n, n, cfg["seed"] + n, smin=1e-6)
+            c_n, w_n = 0.0, 0.0
+            for npl in (n, n // 2):
+                out = run_ref(case("c5", n, n, npl, ALG, seed=0), G, reps=reps + 1)
+                runs = out["reps_timing"][1:]
+                c_n += 0.5 * statistics.median(r[2] for r in runs)
+                w_n += 0.5 * statistics.median(r[0] for r in runs)
+            by_n[n] = {"compute_s": c_n, "wall_s": w_n, "count": cnt}
+            comp_tot += c_n * cnt
+            wall_tot += w_n * cnt
+        line = dict(base, value=len(sizes) / comp_tot, steps=1, steps_requested=args.steps,
+                    ms_per_step=1000.0 * comp_tot,
+                    e2e={"value": len(sizes) / wall_tot, "unit": "matrices/s",
+                         "h2d_bytes_per_step": int((sizes.astype(np.int64) ** 2).sum() * 8),
+                         "d2h_bytes_per_step": int((2 * sizes.astype(np.int64) ** 2 + sizes).sum() * 8),
+                         "api": "reference hypJacL2 per matrix (host buffers; its own allocation and copies)"},
+                    reference={"kind": "reference", "build": REF_BUILD, "by_n": by_n,
+                               "sample": f"one SVD and one HSVD matrix per n, {reps} timed runs each after one "
+                                         "warm-up run; one step = the batch, scaled from the per-n times"})
+    cpu = None
+    if not args.no_cpu:
+        from oracle import oracle as O
+        O.build()
+        cores = os.cpu_count() or 1
+        s0 = O.load_strat(STRAT_PATH, "cycwor", 32)
+        tot, cpu_by = 0.0, {}
+        for n in ns:
             G = synth.make("svd_synth", n, n, cfg["seed"] + n, smin=1e-6)
             s1 = O.load_strat(STRAT_PATH, "cycwor", n // 16)
             per = 0.0
-            for npl in (n, n // 2):           # half SVD, half HSVD
+            for npl in (n, n // 2):
                 t0 = time.perf_counter()
-                r = O.hypjac_l2(ALG, G, npl, s0, s1, nthreads=cores)
+                O.hypjac_l2(ALG, G, npl, s0, s1, nthreads=cores)
                 per += 0.5 * (time.perf_counter() - t0)
             cpu_by[n] = per
-            tot += per * cnt
-        vals.append(len(sizes) / tot)
-    try:
-        from tests.golden.make_golden import HARNESS, case, run_ref
-        if os.path.exists(HARNESS["base"]):
-            tref = 0.0
-            for n in sorted(set(int(x) for x in sizes)):
-                G = synth.make("svd_synth", n, n, cfg["seed"] + n, smin=1e-6)
-                out = run_ref(case("c5", n, n, n, ALG, seed=0), G)
-                ref_by[n] = out["timing"][0]
-                tref += out["timing"][0] * int((sizes == n).sum())
-            ref = {"matrices_per_s_wall": len(sizes) / tref, "s_per_matrix_wall_by_n": ref_by,
-                   "sample": "one SVD per n through the reference's hypJacL2 (oracle/_ref/ref_harness), scaled",
-                   "build": "reference sources, nvcc -arch sm_100a -DUSE_RSQRT -O3"}
-        else:
-            ref = None
-    except Exception as e:  # noqa: BLE001
-        ref = {"error": str(e)[:200]}
-    v = statistics.median(vals)
-    line = {"metric": cfg["metric"], "value": v, "unit": "matrices/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * len(sizes) / v,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "name": "c5", "count": len(sizes), "alg": ALG},
-            "cpu_baseline": {"value": v, "unit": "matrices/s", "cores": cores, "kind": "port",
-                             "sample": "one SVD and one HSVD (NPLUS = n/2) per n by the oracle port, scaled by "
-                                       "the batch's count of each n", "seconds_by_n": cpu_by},
-            "e2e": {"value": v, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    if ref is not None:
-        line["ref_sm100a"] = ref
+            tot += per * int((sizes == n).sum())
+        cpu = {"value": len(sizes) / tot, "unit": "matrices/s", "cores": cores, "kind": "port",
+               "sample": "one SVD and one HSVD (NPLUS = n/2) per n by the oracle port, scaled by the batch's count "
+                         "of each n", "seconds_by_n": cpu_by}
+    if line is None:
+        line = dict(base, value=cpu["value"], steps=1, steps_requested=args.steps, ms_per_step=1000.0 * tot,
+                    e2e={"value": cpu["value"], "unit": "matrices/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0},
+                    note="reference build absent: the CPU oracle port, scaled from one matrix of each n")
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     return 0
 
 
 def reference_arm(args):
+    """The reference's own implementation of the path on this box: its
+    hypJacL2 sources built for sm_100a (oracle/_ref/ref_harness; the
+    reference is GPU code and has no CPU implementation), whole
+    decompositions, timed by the reference's own timer -- value from its
+    compute phase (timing[2]: the device-resident part), e2e from its wall
+    time (timing[0]: allocation, H2D of G, compute, D2H of U, V, D).  The CPU
+    oracle port is reported beside it (cpu_baseline) on a bounded sample."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -337,32 +353,34 @@ def reference_arm(args):
         return reference_arm_batch(args)
     _use(args.config)
     G0 = _input()
-    sweeps = int(os.environ.get("GJX_BENCH_SWEEPS", "0"))
-    ref = None
-    try:
-        ref = ref_gpu_once(G0)
-    except Exception as e:  # noqa: BLE001
-        ref = {"error": str(e)[:200]}
-    if not sweeps:
-        sweeps = (ref or {}).get("sweeps") or 10
-    vals = []
-    samples = []
-    for _ in range(args.warmup):
-        cpu_port_sample(G0, sweeps, min_seconds=2.0)
-    for _ in range(args.steps):
-        c = cpu_port_sample(G0, sweeps, min_seconds=10.0)
-        vals.append(c["value"])
-        samples.append(c)
-    v = statistics.median(vals)
-    line = {"metric": METRIC, "value": v, "unit": "matrices/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": CONFIG,
-            "cpu_baseline": dict(samples[-1], value=v),
-            "e2e": {"value": v, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference has no CPU implementation; its arithmetic is timed through the CPU oracle "
-                    "port (bit-identical restatement); ref_sm100a is the reference's own GPU code"}
+    config = dict(CONFIG, parallelism=("replicas" if args.gpus > 1 else "single GPU"))
+    base = {"metric": METRIC, "unit": "matrices/s", "impl": "reference", "n_gpus": args.gpus, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config}
+    ref = ref_gpu_runs(G0, M, N, NPLUS, ALG, args.steps, args.warmup)
+    sweeps = (ref or {}).get("sweeps") or int(os.environ.get("GJX_BENCH_SWEEPS", "10"))
+    cpu = None if args.no_cpu else cpu_port_sample(G0, sweeps, min_seconds=10.0)
     if ref is not None:
-        line["ref_sm100a"] = ref
+        comp = statistics.median(ref["compute_s"])
+        wall = statistics.median(ref["wall_s"])
+        line = dict(base, value=1.0 / comp, steps=ref["steps"], steps_requested=args.steps,
+                    ms_per_step=1000.0 * comp, step_ms=[1000.0 * x for x in ref["compute_s"]],
+                    sweeps=ref["sweeps"],
+                    e2e={"value": 1.0 / wall, "unit": "matrices/s", "h2d_bytes_per_step": M * N * 8,
+                         "d2h_bytes_per_step": M * N * 8 + (N * N * 8 if ALG & 2 else 0) + N * 8,
+                         "api": "reference hypJacL2 (host buffers; its own allocation and copies)",
+                         "step_ms": [1000.0 * x for x in ref["wall_s"]]},
+                    reference={"kind": "reference", "build": ref["build"], "timer": "the reference's timing[4]",
+                               "rot_s": ref["rot_s"], "rot_b": ref["rot_b"]})
+    else:  # no reference build on this host: the oracle port, one sampled outer step per step
+        per_step = cpu["seconds"] / cpu["outer_steps"]
+        line = dict(base, value=cpu["value"], steps=cpu["outer_steps"], steps_requested=args.steps,
+                    ms_per_step=1000.0 * per_step,
+                    e2e={"value": cpu["value"], "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                    note="reference build absent: the CPU oracle port, one step = one sampled outer step "
+                         f"({PAIRS} block pairs); value scaled to a whole decomposition")
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     return 0
 
@@ -401,6 +419,21 @@ def batch_inputs(sizes, dev, seed: int = 5000):
     return buf, offs
 
 
+def shard_batch(G_all, offs_all, sizes, rank: int, world: int):
+    """This rank's shard of one batch (strong scaling): the matrices the
+    size-balanced partition gives it (indices `mine`, ascending), their sizes,
+    their offsets in the shard and the shard's buffer (their G, each column
+    major with ld = n, back to back).  G_all holds the whole batch, matrix b
+    at [offs_all[b], offs_all[b + 1])."""
+    import torch
+    from gpujachx_b200 import batch as B
+    mine = B.partition(sizes, sizes, world)[rank]
+    sz = sizes[mine]
+    offs = np.concatenate([[0], np.cumsum(sz.astype(np.int64) ** 2)])
+    G = torch.cat([G_all[int(offs_all[b]):int(offs_all[b + 1])] for b in mine])
+    return mine, sz, offs, G
+
+
 def batch_flops_bytes(sizes, sweeps, full=True):
     """Algorithmic FLOP and bytes of the sweeps each matrix ran (reference
     geometry, w = 32; P_sweep = n1 (n1 - 1) / 2 cyclic block pairs)."""
@@ -431,12 +464,8 @@ def main_batch(args):
     sizes = batch_sizes(cfg["count"], cfg["seed"])
     if args.shard and world > 1:
         # strong scaling: one batch, split by the size-balanced partition
-        from gpujachx_b200 import batch as B
         G_all, offs_all = batch_inputs(sizes, dev, cfg["seed"])
-        mine = B.partition(sizes, sizes, world)[rank]
-        sizes = sizes[mine]
-        offs = np.concatenate([[0], np.cumsum(sizes.astype(np.int64) ** 2)])
-        G0 = torch.cat([G_all[int(offs_all[b]):int(offs_all[b + 1])] for b in mine])
+        mine, sizes, offs, G0 = shard_batch(G_all, offs_all, sizes, rank, world)
         del G_all
     else:
         # weak scaling: every rank solves its own batch of the same shapes
@@ -652,7 +681,7 @@ def main():
     ach = BYTES_PER_PAIR * PAIRS / l1_mean_s / 1e9
     flops = FLOP_PER_PAIR * PAIRS / l1_mean_s / 1e12
     roof = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-            "traffic": _profiled_traffic() if args.config == "c2" else None,
+            "traffic": RECORDED_TRAFFIC.get(args.config),
             "kernel": "gjx::%s<%s,%s,%d>" % ("l1_sweep_kernel" if one_launch else "l1_step_kernel",
                                              "true" if ALG & 1 else "false", "true" if ALG & 2 else "false",
                                              tuned["split"]),
@@ -663,7 +692,7 @@ def main():
             "algorithmic_bytes_per_launch": BYTES_PER_PAIR * PAIRS,
             "algorithmic_flop_per_launch": FLOP_PER_PAIR * PAIRS, "fp64_tflops": flops,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
-                              "workload (cold L2), recorded in profiles/l1_step_kernel_svd4096x2048.md"}
+                              "workload (cold L2), recorded from one capture (bench.RECORDED_TRAFFIC)"}
 
     # e2e through the public host API (pinned buffers, H2D + D2H inside)
     pin = torch.empty((N, M), dtype=torch.float64, pin_memory=True).numpy().T  # Fortran view

@@ -56,14 +56,27 @@ def _run(cmd, verbose):
 
 
 def build_lib(force: bool = False, verbose: bool = True) -> str:
+    """Each source compiled to its own object (in parallel), then linked."""
     srcs = [os.path.join(CSRC, s) for s in LIB_SOURCES]
-    deps = srcs + glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + [
+    hdrs = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + [
         os.path.join(ROOT, "include", "gjx.h")]
-    if not force and not _newer(LIB, deps):
+    if not force and not _newer(LIB, srcs + hdrs):
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
+    objdir = os.path.join(LIBDIR, "obj")
+    os.makedirs(objdir, exist_ok=True)
+
+    def one(src):
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        if force or _newer(obj, [src] + hdrs):
+            _run(["nvcc"] + NVCC_FLAGS + ["-c", "-o", obj + ".tmp", src], verbose)
+            os.replace(obj + ".tmp", obj)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(srcs)) as ex:
+        objs = list(ex.map(one, srcs))
     tmp = LIB + ".tmp"
-    _run(["nvcc"] + NVCC_FLAGS + ["-shared", "-o", tmp] + srcs + ["-ldl"], verbose)
+    _run(["nvcc"] + ARCH + ["-shared", "-o", tmp] + objs + ["-ldl"], verbose)
     os.replace(tmp, LIB)
     return LIB
 
@@ -92,20 +105,21 @@ def build_pp(force: bool = False, verbose: bool = True) -> str:
     return PP
 
 
-def build_strat(ref_root: str = "/root/reference", force: bool = False, verbose: bool = True) -> str:
+def build_strat(ref_root: str | None = None, force: bool = False, verbose: bool = True) -> str:
     """Compile the reference's strategy-table headers, where they lie, into strat.so.
 
     The headers are data (``unsigned char|short <family>NNNNN[S][N/2][2] = {...}``);
     they are consumed unchanged, as the reference's own strat/proc_*-lnx.sh
     does, with the same exported symbol names.
     """
-    sdir = os.path.join(ref_root, "strat")
+    ref_root = ref_root or os.environ.get("GJX_REF_ROOT", "")
+    sdir = os.path.join(ref_root, "strat") if ref_root else ""
     if not force and os.path.exists(STRAT):
         return STRAT
-    if not os.path.isdir(sdir):
+    if not sdir or not os.path.isdir(sdir):
         if os.path.exists(STRAT):
             return STRAT
-        raise FileNotFoundError(f"no strategy tables under {sdir} and no prebuilt {STRAT}")
+        raise FileNotFoundError(f"no strategy tables (set GJX_REF_ROOT to the reference tree) and no prebuilt {STRAT}")
     os.makedirs(LIBDIR, exist_ok=True)
     work = tempfile.mkdtemp(prefix="gjx_strat_")
     try:
@@ -133,7 +147,7 @@ def build_strat(ref_root: str = "/root/reference", force: bool = False, verbose:
 
 def build_all(force: bool = False, verbose: bool = True):
     build_lib(force=force, verbose=verbose)
-    build_strat(force=False, verbose=verbose)
+    build_strat(force=False, verbose=verbose)  # tables from $GJX_REF_ROOT/strat
     build_x1(force=force, verbose=verbose)
     build_pp(force=force, verbose=verbose)
 

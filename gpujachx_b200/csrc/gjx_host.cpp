@@ -645,11 +645,15 @@ size_t noalloc_scratch_need()
 int noalloc_sweeps(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
                    double *const dG, const unsigned lddG, double *const dV, const unsigned lddV, double *const dD,
                    void *const stream, void *const scratch, const size_t scratch_bytes, const int dev,
-                   unsigned *const glbSwp, unsigned long long *const glb_s, unsigned long long *const glb_b)
+                   const unsigned long long ctx, unsigned *const glbSwp, unsigned long long *const glb_s,
+                   unsigned long long *const glb_b)
 {
+  // what the scratch of a device holds; a new context (id ctx, 0 if unknown)
+  // means a new, zeroed array and unconfigured kernels: everything again
   struct Uploaded {
     const void *scratch = nullptr;
     unsigned long long version = ~0ull;
+    unsigned long long ctx = 0u;
     bool configured = false;
   };
   static std::vector<Uploaded> up; // per device: what the scratch holds
@@ -669,6 +673,11 @@ int noalloc_sweeps(const unsigned routine, const unsigned nrow, const unsigned n
   Uploaded &u = up[(size_t)dev];
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
   unsigned char *const base = static_cast<unsigned char *>(scratch);
+  if (u.ctx != ctx || !ctx) {
+    u.configured = false;
+    u.scratch = nullptr;
+    u.ctx = ctx;
+  }
   if (!u.configured) {
     GJX_CUDA(l1_configure(), "l1_configure");
     u.configured = true;

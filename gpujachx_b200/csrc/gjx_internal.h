@@ -104,7 +104,7 @@ cudaError_t launch_initV(double *V, unsigned ncol, unsigned ldV, cudaStream_t s)
 size_t noalloc_scratch_need();
 int noalloc_sweeps(unsigned routine, unsigned nrow, unsigned ncol, unsigned nplus, double *dG, unsigned lddG,
                    double *dV, unsigned lddV, double *dD, void *stream, void *scratch, size_t scratch_bytes, int dev,
-                   unsigned *glbSwp, unsigned long long *glb_s, unsigned long long *glb_b);
+                   unsigned long long ctx, unsigned *glbSwp, unsigned long long *glb_s, unsigned long long *glb_b);
 int check_dev_args(unsigned routine, unsigned nrow, unsigned ncol, unsigned nplus, const double *dG, unsigned lddG,
                    const double *dV, unsigned lddV, const double *dD, const unsigned *glbSwp,
                    const unsigned long long *glb_s, const unsigned long long *glb_b);

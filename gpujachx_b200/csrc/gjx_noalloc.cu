@@ -16,12 +16,19 @@
 // name is only a host-side stand-in, not a device address, so the address is
 // taken with cudaGetSymbolAddress, once per device, with that device current,
 // on the first call made on it; that first call should come before any stream
-// capture.  All calls share the array and it keeps the last call's contents:
-// the counters are cleared by each call, the tables are rewritten whenever
-// the loaded tables or the device change.  Calls that overlap on the GPU
-// (other streams, other host threads on the same device) race on it.
+// capture.  The set-up is repeated only when the device's CUDA context is not
+// the one it was made in (a caller's cudaDeviceReset destroys the context, and
+// the array and its address with it): the context's id is kept beside the
+// address, and the tables are uploaded again into the new array.  All calls
+// share the array and it keeps the last call's contents: the counters are
+// cleared by each call, the tables are rewritten whenever the loaded tables,
+// the device or its context change.  Calls that overlap on the GPU (other
+// streams, other host threads on the same device) race on it; calls from host
+// threads are serialised by the library's lock for their whole duration.
 #include <mutex>
 #include <vector>
+
+#include <cudaTypedefs.h>
 
 #include "gjx.h"
 #include "gjx_internal.h"
@@ -34,7 +41,34 @@ constexpr size_t kScratchBytes = 520u * 1024u;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 std::mutex g_sym_mtx;
-std::vector<void *> g_sym; // per device: the device address of g_noalloc_scratch
+struct SymAddr {
+  void *ptr = nullptr;         // device address of g_noalloc_scratch
+  unsigned long long ctx = 0u; // id of the context it belongs to (0: none yet)
+};
+std::vector<SymAddr> g_sym; // per device
+
+// id of the calling thread's current context (cuCtxGetId, unique for the life
+// of the process), 0 if it cannot be had
+unsigned long long current_ctx_id()
+{
+  static PFN_cuCtxGetCurrent_v4000 get_cur = nullptr;
+  static PFN_cuCtxGetId_v12000 get_id = nullptr;
+  if (!get_cur || !get_id) {
+    void *f1 = nullptr, *f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2)
+      return 0u;
+    get_cur = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(f1);
+    get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(f2);
+  }
+  CUcontext c = nullptr;
+  unsigned long long id = 0u;
+  if (get_cur(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS)
+    return 0u;
+  return id;
+}
 
 } // namespace
 
@@ -59,21 +93,30 @@ extern "C" int gjx_hypJacL2_noalloc(const unsigned routine, const unsigned nrow,
     gjx::set_error(cudaGetErrorString(e));
     return GJX_ERR_CUDA;
   }
+  // makes the device's primary context current on this thread (no allocation)
+  e = cudaSetDevice(dev);
+  if (e != cudaSuccess) {
+    gjx::set_error(cudaGetErrorString(e));
+    return GJX_ERR_CUDA;
+  }
+  const unsigned long long ctx = current_ctx_id();
   void *ptr = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_sym_mtx);
     if ((size_t)dev >= g_sym.size())
-      g_sym.resize((size_t)dev + 1u, nullptr);
-    if (!g_sym[(size_t)dev]) { // set-up, once per device, with that device current
+      g_sym.resize((size_t)dev + 1u);
+    SymAddr &a = g_sym[(size_t)dev];
+    if (!a.ptr || a.ctx != ctx || !ctx) { // set-up, once per device and context, with that device current
       e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
       if (e != cudaSuccess) {
         gjx::set_error(cudaGetErrorString(e));
         return GJX_ERR_CUDA;
       }
-      g_sym[(size_t)dev] = ptr;
+      a.ptr = ptr;
+      a.ctx = ctx;
     }
-    ptr = g_sym[(size_t)dev];
+    ptr = a.ptr;
   }
   return gjx::noalloc_sweeps(routine, nrow, ncol, nplus, dG, lddG, dV, lddV, dD, stream, ptr, kScratchBytes, dev,
-                             glbSwp, glb_s, glb_b);
+                             ctx, glbSwp, glb_s, glb_b);
 }

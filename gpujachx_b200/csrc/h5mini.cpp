@@ -234,7 +234,17 @@ public:
       return fail(err, "not a dataset");
     if (!dataspace(*sp, a.dims, err) || !datatype(*ty, a, err))
       return false;
-    const uint64_t need = a.count() * a.size;
+    // the byte count must not wrap: every extent defined, and the product of
+    // the extents and the element size no larger than the file (a dataset
+    // stored in the file cannot be longer than the file)
+    uint64_t need = a.size;
+    for (const uint64_t d : a.dims) {
+      if (d == kUndef)
+        return fail(err, "dataset with an undefined extent");
+      if (d && need > len_ / d)
+        return fail(err, "dataset larger than the file");
+      need *= d;
+    }
     uint64_t daddr = kUndef, dsize = 0u;
     const uint8_t *compact = nullptr;
     if (!layout(*ly, (unsigned)a.dims.size(), daddr, dsize, compact, err))

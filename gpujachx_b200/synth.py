@@ -8,6 +8,10 @@ thread while generating so that the QR factors are reproducible).
 * :func:`svd_synth` -- Q1 diag(s) Q2^T, Haar Q1/Q2, s geometric from 1 to smin
                        (configs 1 and 4, the batch of config 5)
 * :func:`graded`    -- B diag(d), B i.i.d. N(0,1), d_j = 10^U(lo, 0) (config 3)
+* :func:`haar_gpu`  -- Q1 diag(s) Q2^T formed on the GPU (torch CUDA generator):
+                       the 8192 x 8192 configuration is too large for a host QR
+                       at start-up; the same seed gives the same bits with the
+                       same torch / CUDA build on a B200
 """
 
 from __future__ import annotations
@@ -58,12 +62,27 @@ def graded(m: int, n: int, seed: int, lo: float = -6.0) -> np.ndarray:
     return np.asfortranarray(B * d)
 
 
+def haar_gpu(m: int, n: int, seed: int, smin: float = 1e-12) -> np.ndarray:
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+
+    def haar(k):
+        q, r = torch.linalg.qr(torch.randn((k, k), dtype=torch.float64, device=dev, generator=gen))
+        return q * torch.sign(torch.diagonal(r)).unsqueeze(0)
+
+    sv = torch.logspace(0.0, float(np.log10(smin)), n, dtype=torch.float64, device=dev)
+    G = (haar(m)[:, :n] * sv) @ haar(n).T
+    return np.asfortranarray(G.cpu().numpy())
+
+
 def digest(a) -> str:
     """sha256 of the bytes of a float64 array in Fortran order."""
     return hashlib.sha256(np.asfortranarray(a, dtype=np.float64).tobytes(order="F")).hexdigest()
 
 
-GENERATORS = {"gaussian": gaussian, "svd_synth": svd_synth, "graded": graded}
+GENERATORS = {"gaussian": gaussian, "svd_synth": svd_synth, "graded": graded, "haar_gpu": haar_gpu}
 
 
 def make(gen: str, m: int, n: int, seed: int, **kw) -> np.ndarray:

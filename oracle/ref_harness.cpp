@@ -5,8 +5,12 @@
 // golden fixtures in tests/golden/ are its outputs).  It mirrors the
 // argument handling of the reference CLI 1/main.cu:10-160 without HDF5:
 //
-//   ref_harness DEV SDY SNP0 SNP1 ALG NPLUS M N IN.bin OUT.bin
+//   ref_harness DEV SDY SNP0 SNP1 ALG NPLUS M N IN.bin OUT.bin [REPS]
 //
+// REPS (default 1) runs hypJacL2 that many times on the same input (G
+// restored before each run) and prints one line per run to stdout,
+// "REP r ret sweeps wall setup compute cleanup" (the reference's timing[4],
+// seconds); OUT.bin holds the last run.
 // IN.bin : M*N doubles, Fortran order, LDA = M.
 // OUT.bin: int32 ret, uint32 sweeps, uint64 rot_s, uint64 rot_b,
 //          double timing[4], double G[M*N], double V[N*N] (ALG & 2), double D[N].
@@ -28,8 +32,8 @@ extern "C" int hypJacL2(const unsigned routine, const unsigned nrow, const unsig
 
 int main(int argc, char **argv)
 {
-  if (argc != 11) {
-    std::fprintf(stderr, "%s DEV SDY SNP0 SNP1 ALG NPLUS M N IN.bin OUT.bin\n", argv[0]);
+  if (argc != 11 && argc != 12) {
+    std::fprintf(stderr, "%s DEV SDY SNP0 SNP1 ALG NPLUS M N IN.bin OUT.bin [REPS]\n", argv[0]);
     return EXIT_FAILURE;
   }
   const int dev = std::atoi(argv[1]);
@@ -37,6 +41,9 @@ int main(int argc, char **argv)
   const unsigned nplus = (unsigned)std::atoi(argv[6]);
   const unsigned m = (unsigned)std::atoi(argv[7]);
   const unsigned n = (unsigned)std::atoi(argv[8]);
+  const int reps = (argc == 12) ? std::atoi(argv[11]) : 1;
+  if (reps < 1)
+    return EXIT_FAILURE;
 
   init_strats(argv[2], argv[3], 32u, argv[4], (n + 15u) / 16u);
   if (configureGPU(dev) < 30)
@@ -54,12 +61,22 @@ int main(int argc, char **argv)
   if (!f || std::fread(hG, sizeof(double), (size_t)m * n, f) != (size_t)m * n)
     return EXIT_FAILURE;
   std::fclose(f);
+  std::vector<double> g0;
+  if (reps > 1)
+    g0.assign(hG, hG + (size_t)m * n);
 
   unsigned swp = 0u;
   unsigned long long s = 0ull, b = 0ull;
   double timing[4] = {0.0, 0.0, 0.0, 0.0};
-  // as 1/main.cu:78-80: V is allocated with the leading dimension of G
-  const int ret = hypJacL2(alg, m, n, nplus, hG, m, hV, (alg & 2u) ? m : 0u, hD, &swp, &s, &b, timing);
+  int ret = 0;
+  for (int r = 0; r < reps; ++r) {
+    if (r)
+      std::memcpy(hG, g0.data(), sizeof(double) * g0.size());
+    // as 1/main.cu:78-80: V is allocated with the leading dimension of G
+    ret = hypJacL2(alg, m, n, nplus, hG, m, hV, (alg & 2u) ? m : 0u, hD, &swp, &s, &b, timing);
+    if (reps > 1)
+      std::printf("REP %d %d %u %.9f %.9f %.9f %.9f\n", r, ret, swp, timing[0], timing[1], timing[2], timing[3]);
+  }
 
   f = std::fopen(argv[10], "wb");
   if (!f)

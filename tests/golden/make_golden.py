@@ -7,7 +7,12 @@ records its outputs: sha256 of U, V, D, the full D, the sweep and rotation
 counts.  It needs a B200 (the reference is GPU code), so it runs on the GPU
 host:
 
-    python tests/golden/make_golden.py [OUT.json] [--variant base|qr|drmac]
+    python tests/golden/make_golden.py [OUT.json] [--variant base|qr|drmac] [--large]
+
+--large records the benchmark-size cases (LARGE_CASES: the 8192 x 8192
+configuration, one SVD and one HSVD matrix of each batch size 64..512, the
+4096 x 2048 and 2048 x 1024 configurations) into ref_golden_large.json:
+digests and counts only (the 8192 x 8192 input is formed on the GPU).
 
 The committed tests/golden/ref_golden*.json came from this script; the tests
 regenerate each input, check its sha256, and compare the oracle (CPU) and the
@@ -77,6 +82,18 @@ CASES = [
 ]
 
 
+# Benchmark-size cases: the reference takes about a minute on the first.
+LARGE_CASES = [
+    case("c4_8192_alg11", 8192, 8192, 8192, 11, gen="haar_gpu", seed=1003, smin=1e-12),
+    case("c2_4096x2048_alg11", 4096, 2048, 2048, 11, seed=1001),
+    case("c3_2048x1024_np512_alg11", 2048, 1024, 512, 11, gen="graded", seed=1002),
+    case("c1_256_alg11_np128", 256, 256, 128, 11, gen="svd_synth", seed=1000, smin=1e-8),
+] + [
+    case("c5_n%d_%s" % (n, "svd" if p == n else "hsvd"), n, n, p, 11, gen="svd_synth", seed=5000 + n, smin=1e-6)
+    for n in range(64, 513, 64) for p in (n, n // 2)
+]
+
+
 def make_input(c):
     if c["gen"] == "orth":  # orthonormal columns scaled by powers of two: no rotation at all
         Q = synth.svd_synth(c["m"], c["n"], c["seed"], smin=1.0)
@@ -84,15 +101,18 @@ def make_input(c):
     return synth.make(c["gen"], c["m"], c["n"], c["seed"], **c["kw"])
 
 
-def run_ref(c, G, variant="base", dev=0):
+def run_ref(c, G, variant="base", dev=0, reps=1, timeout=600):
+    """One process of the reference harness on G: `reps` runs of its
+    hypJacL2 (the output is the last run's); "reps_timing" lists each run's
+    timing[4] (wall, setup + H2D, compute, D2H + cleanup; seconds)."""
     m, n = c["m"], c["n"]
     with tempfile.TemporaryDirectory() as d:
         fin, fout = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
         with open(fin, "wb") as f:
             f.write(np.asfortranarray(G).tobytes("F"))
         cmd = [HARNESS[variant], str(dev), STRAT, c["snp0"], c["snp1"], str(c["alg"]), str(c["nplus"]),
-               str(m), str(n), fin, fout]
-        p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+               str(m), str(n), fin, fout] + ([str(reps)] if reps > 1 else [])
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
         if p.returncode != 0:
             raise RuntimeError(f"reference failed on {c['name']}: {p.stdout[-500:]} {p.stderr[-500:]}")
         raw = open(fout, "rb").read()
@@ -112,14 +132,16 @@ def run_ref(c, G, variant="base", dev=0):
     U = take(np.float64, m * n).reshape(n, m).T
     V = take(np.float64, n * n).reshape(n, n).T if (c["alg"] & 2) else None
     D = take(np.float64, n).copy()
+    reps_timing = [[float(x) for x in ln.split()[4:8]] for ln in p.stdout.splitlines() if ln.startswith("REP ")]
     return dict(ret=ret, sweeps=swp, rot_s=rs, rot_b=rb, timing=timing.tolist(), U=U, V=V, D=D,
-                stdout=p.stdout)
+                stdout=p.stdout, reps_timing=reps_timing or [timing.tolist()])
 
 
 def record(c, out):
     r = dict(ret=out["ret"], sweeps=out["sweeps"], rot_s=out["rot_s"], rot_b=out["rot_b"],
-             U_sha=synth.digest(out["U"]), D_sha=synth.digest(out["D"]),
-             D=[float(x).hex() for x in out["D"]])
+             U_sha=synth.digest(out["U"]), D_sha=synth.digest(out["D"]))
+    if len(out["D"]) <= 512:
+        r["D"] = [float(x).hex() for x in out["D"]]
     if out["V"] is not None:
         r["V_sha"] = synth.digest(out["V"])
     return r
@@ -131,10 +153,11 @@ def main():
     if "--variant" in sys.argv:
         variant = sys.argv[sys.argv.index("--variant") + 1]
         args = [a for a in args if a != variant]
+    large = "--large" in sys.argv
     out_path = args[0] if args else os.path.join(os.path.dirname(os.path.abspath(__file__)),
-                                                f"ref_golden_{variant}.json")
+                                                f"ref_golden_{'large' if large else variant}.json")
     res = []
-    for c in CASES:
+    for c in (LARGE_CASES if large else CASES):
         G = make_input(c)
         o = run_ref(c, G, variant)
         entry = dict(c)

@@ -172,3 +172,18 @@ def test_reader_newer_format(built, tmp_path):
     assert np.array_equal(h5.read(str(f), "sub/B", as_float=False), ints.astype(np.int32))
     with pytest.raises(GjxError, match="classic-format"):
         h5.write(str(f), "g", {"A": np.ones(1)}, mode=2)
+
+
+def test_dataset_extents_that_overflow_are_refused(built, tmp_path):
+    """A file whose dataspace claims extents whose byte count wraps around 2^64
+    (here 2^62 x 2^4 doubles) is refused with a message, not read."""
+    f = tmp_path / "wrap.h5"
+    h5.write(str(f), "g", {"A": np.ones((3, 7))}, mode=0)
+    raw = bytearray(f.read_bytes())
+    dims = struct.pack("<QQ", 3, 7)
+    at = raw.find(dims)
+    assert at > 0
+    raw[at:at + 16] = struct.pack("<QQ", 1 << 62, 1 << 4)
+    f.write_bytes(bytes(raw))
+    with pytest.raises(GjxError, match="larger than the file"):
+        h5.read(str(f), "g/A")

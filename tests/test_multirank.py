@@ -92,3 +92,51 @@ def test_batch_shards_over_two_gloo_ranks():
     assert s0 == s1 == float(sum(range(4096)))
     assert not set(m0) & set(m1) and len(set(m0) | set(m1)) == 4096
     assert imb < 1.001
+
+
+def _shard_data_rank(rank, world, port, q):
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import bench
+    sizes = bench.batch_sizes(96, 5000)               # the c5 size distribution, a small batch
+    offs = np.concatenate([[0], np.cumsum(sizes.astype(np.int64) ** 2)])
+    G_all = torch.arange(int(offs[-1]), dtype=torch.float64)   # every element its own index
+    mine, sz, soffs, G = bench.shard_batch(G_all, offs, sizes, rank, world)
+    parts = [None] * world
+    dist.all_gather_object(parts, (mine.tolist(), sz.tolist(), soffs.tolist(), G.numpy()))
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank == 0:
+        q.put((sizes.tolist(), offs.tolist(), parts))
+
+
+def test_sharded_batch_reassembles_over_two_gloo_ranks():
+    """bench.py --shard: each rank slices its shard out of the same batch;
+    the shards are disjoint, cover the batch, and their buffers put back in
+    index order give the batch buffer bit for bit."""
+    import numpy as np
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 33600 + (os.getpid() % 2000)
+    ps = [ctx.Process(target=_shard_data_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    sizes, offs, parts = q.get(timeout=120)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    idx = sorted(i for mine, *_ in parts for i in mine)
+    assert idx == list(range(len(sizes)))             # disjoint and complete
+    whole = np.empty(offs[-1])
+    for mine, sz, soffs, G in parts:
+        assert sz == [sizes[i] for i in mine]
+        assert soffs[-1] == len(G)
+        for k, b in enumerate(mine):
+            whole[offs[b]:offs[b + 1]] = G[soffs[k]:soffs[k + 1]]
+    assert np.array_equal(whole, np.arange(offs[-1], dtype=np.float64))
+    loads = [sum(s * s * s for s in sz) for _, sz, _, _ in parts]
+    assert max(loads) / (sum(loads) / 2) < 1.05       # balanced by work

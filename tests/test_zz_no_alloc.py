@@ -86,3 +86,35 @@ def test_noalloc_refuses_tables_beyond_its_scratch(built):
     # argument errors keep the reference's codes
     assert L.gjx_hypJacL2_noalloc(16, 64, 32, 32, fake, 64, None, 0, fake, None, ctypes.byref(swp), ctypes.byref(s),
                                   ctypes.byref(b)) == -1
+
+
+@pytest.mark.gpu
+def test_noalloc_second_call_takes_no_device_memory(built):
+    """Once the first call on a device has set up the static array, a call
+    changes the device's free memory by nothing: every cudaMalloc (the
+    library's or a caching allocator's) would take at least one 2 MiB page."""
+    import torch
+    import gpujachx_b200 as g
+    L = g.lib()
+    c = case("na_mem", 1024, 512, 512, 11, seed=504)
+    G = make_input(c)
+    g.init_strats(None, "cycwor", 32, "cycwor", c["n"] // 16)
+    m, n = G.shape
+    dG = torch.tensor(np.ascontiguousarray(G.T), dtype=torch.float64, device="cuda")
+    dG0 = dG.clone()
+    dV = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    dD = torch.empty(n, dtype=torch.float64, device="cuda")
+    swp, s, b = ctypes.c_uint(), ctypes.c_ulonglong(), ctypes.c_ulonglong()
+
+    def call():
+        dG.copy_(dG0)
+        torch.cuda.synchronize()
+        return L.gjx_hypJacL2_noalloc(11, m, n, 512, dG.data_ptr(), m, dV.data_ptr(), n, dD.data_ptr(), None,
+                                      ctypes.byref(swp), ctypes.byref(s), ctypes.byref(b))
+
+    assert call() == 0, g.last_error()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    assert call() == 0, g.last_error()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
