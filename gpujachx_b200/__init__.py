@@ -75,6 +75,8 @@ def lib() -> ctypes.CDLL:
     L.gjx_hypJacL2_dev.restype = i
     L.gjx_hypJacL2_noalloc.argtypes = L.gjx_hypJacL2_dev.argtypes
     L.gjx_hypJacL2_noalloc.restype = i
+    L.gjx_hypJacL2_split.argtypes = L.gjx_hypJacL2_dev.argtypes
+    L.gjx_hypJacL2_split.restype = i
     L.gjx_release_cache.argtypes = []
     L.gjx_release_cache.restype = i
     L.gjx_set_verbose.argtypes = [i]
@@ -248,6 +250,28 @@ def hypJacL2_dev(routine: int, G, nplus: int, V=None, D=None, stream=None, nrow:
     ret = lib().gjx_hypJacL2_dev(routine, nrow, ncol, nplus, G.data_ptr(), lddG,
                                  V.data_ptr() if full else None, V.shape[1] if full else 0,
                                  D.data_ptr(), st, ctypes.byref(swp), ctypes.byref(s), ctypes.byref(b))
+    if check and ret:
+        raise GjxError(ret, last_error() if ret > 0 else "invalid argument")
+    return ret, swp.value, s.value, b.value
+
+
+def hypJacL2_split(routine: int, G, nplus: int, V=None, D=None, stream=None, nrow: Optional[int] = None,
+                   check: bool = True):
+    """The split-precision form on device-resident torch tensors, in place,
+    with the arguments of hypJacL2_dev: the Gram matrices and the updates of
+    G and V run as exact int8 slice products on the tensor cores (blocks of
+    32 columns, pairs of 64; ncol a multiple of 64).  Not bit-identical to
+    the plain form: its accuracy is reported against an FP64 reference.
+    Returns (ret, sweeps, rot_s, rot_b)."""
+    ncol, lddG = G.shape
+    nrow = lddG if nrow is None else nrow
+    full = bool(routine & FULL_SVD)
+    swp = ctypes.c_uint(0)
+    s, b = ctypes.c_ulonglong(0), ctypes.c_ulonglong(0)
+    st = stream.cuda_stream if stream is not None else None
+    ret = lib().gjx_hypJacL2_split(routine, nrow, ncol, nplus, G.data_ptr(), lddG,
+                                   V.data_ptr() if full else None, V.shape[1] if full else 0,
+                                   D.data_ptr(), st, ctypes.byref(swp), ctypes.byref(s), ctypes.byref(b))
     if check and ret:
         raise GjxError(ret, last_error() if ret > 0 else "invalid argument")
     return ret, swp.value, s.value, b.value

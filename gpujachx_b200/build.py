@@ -36,7 +36,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
                      "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 
-LIB_SOURCES = ["gjx_kernels.cu", "gjx_host.cpp", "gjx_noalloc.cu", "gjx_h5abi.cpp", "h5mini.cpp"]
+LIB_SOURCES = ["gjx_kernels.cu", "gjx_split.cu", "gjx_host.cpp", "gjx_noalloc.cu", "gjx_h5abi.cpp", "h5mini.cpp"]
 X1_SOURCES = ["x1.cpp"]
 
 STRAT_FAMILIES = ["mmstep", "BrentL", "colcyc", "cycloc", "rowcyc", "cycwor"]

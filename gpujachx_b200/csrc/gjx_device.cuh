@@ -56,7 +56,7 @@ __device__ __forceinline__ double pow2(const int k) { return __longlong_as_doubl
 //     midpoint (2Y+1) * 2^-54 iff (2Y+1)^2 * F < 2^160, F = f 2^52, decided
 //     in integers.
 // Any correctly rounded 1/sqrt returns these bits.
-__device__ __noinline__ long long rsqrt_fix_exact(long long Y, const unsigned long long F)
+static __device__ __noinline__ long long rsqrt_fix_exact(long long Y, const unsigned long long F)
 {
   for (int i = 0; (i < 4) && above_mid((unsigned long long)(2 * Y + 1), F); ++i)
     ++Y;
@@ -66,7 +66,7 @@ __device__ __noinline__ long long rsqrt_fix_exact(long long Y, const unsigned lo
 }
 
 // the whole method, every input class; the slow path of rsqrt_rn below
-__device__ __noinline__ double rsqrt_rn_full(const double a)
+static __device__ __noinline__ double rsqrt_rn_full(const double a)
 {
   unsigned long long bits = (unsigned long long)__double_as_longlong(a);
   if ((bits >> 63) || ((bits >> 52) == 0x7FFu) || !(bits << 1)) { // negative, inf, nan, zero
@@ -193,6 +193,76 @@ __device__ __forceinline__ int rotH(const double Apq, const double Dp, const dou
   c = large ? 1.0 : (mid ? cr : kCoshIFix);
   t = (large || mid) ? tt : kTanh1Fix;
   return large ? 0 : (mid ? (cr > 1.0) : 1);
+}
+
+// one inner rotation, as the lanes that compute it hand it to those that apply it
+struct Rot {
+  double c, t, t_;
+  int mode; // 0 nothing, 1 rotate, 2 swap columns
+  int scale, swap;
+};
+
+// rotT (trig) or rotH; when the two halves of the warp need different kinds,
+// both are computed and selected, so the warp does not run them one after
+// the other (each is a long dependent chain of divisions and square roots)
+__device__ __forceinline__ int rot_either(const bool trig, const double Apq, const double Dp, const double Dq,
+                                          double &c, double &t)
+{
+  if (__all_sync(0xffffffffu, trig))
+    return rotT(Apq, Dp, Dq, c, t);
+  if (__all_sync(0xffffffffu, !trig))
+    return rotH(Apq, Dp, Dq, c, t);
+  double c1, t1, c2, t2;
+  const int b1 = rotT(Apq, Dp, Dq, c1, t1), b2 = rotH(Apq, Dp, Dq, c2, t2);
+  c = trig ? c1 : c2;
+  t = trig ? t1 : t2;
+  return trig ? b1 : b2;
+}
+
+template <bool SORT>
+__device__ __forceinline__ Rot inner_rot(const double Dp, const double Dq, const double Apq, const unsigned p,
+                                         const unsigned q, const int definite, const unsigned npos, unsigned &ts_out,
+                                         unsigned &tb_out)
+{
+  // branch-free: the two half-warps handle different pairs, so every choice
+  // below is a select of values computed by both (no divergent paths)
+  Rot r;
+  const double Dp_ = __dsqrt_rn(Dp), Dq_ = __dsqrt_rn(Dq), Apq_ = fabs(Apq), Dpq_ = Dp_ * Dq_;
+  const int ts = !(Apq_ < (Dpq_ * kMyTol));
+  int tb;
+  if (!SORT) {
+    // the rotation is computed whether or not it is applied (no side
+    // effects), so that its latency overlaps the relative test
+    const bool trig = definite || ((p < npos) && (q < npos)) || ((p >= npos) && (q >= npos));
+    double c, t;
+    const int b = rot_either(trig, Apq, Dp, Dq, c, t);
+    r.c = ts ? c : 1.0;
+    r.t = ts ? t : 0.0;
+    r.t_ = ts ? (trig ? -t : t) : 0.0;
+    tb = ts ? b : 0;
+    r.mode = ts;
+    r.scale = tb;
+    r.swap = 0;
+  }
+  else {
+    const int def = definite ? definite : ((p < npos) && (q < npos)) ? +1 : ((p >= npos) && (q >= npos)) ? -1 : 0;
+    double c, t;
+    const int b = rot_either(def != 0, Apq, Dp, Dq, c, t);
+    const double t_ = def ? -t : t;
+    const double Dp2 = __fma_rn(t, Apq, Dp), Dq2 = __fma_rn(t_, Apq, Dq); // used when ts and def
+    const int swp = !((!def) || ((def > 0) && (Dp2 >= Dq2)) || ((def < 0) && (Dp2 <= Dq2)));
+    const int order = ((def > 0) && (Dp < Dq)) || ((def < 0) && (Dq < Dp));
+    r.c = ts ? c : 1.0;
+    r.t = ts ? t : 0.0;
+    r.t_ = ts ? t_ : 0.0;
+    tb = ts ? b : 0;
+    r.mode = ts ? 1 : (order ? 2 : 0);
+    r.scale = tb;
+    r.swap = ts ? swp : 0;
+  }
+  ts_out = (unsigned)ts;
+  tb_out = (unsigned)tb;
+  return r;
 }
 
 // ---------------------------------------------------------------------------

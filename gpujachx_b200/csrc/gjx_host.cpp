@@ -42,7 +42,7 @@ struct Strat {
   std::vector<uint8_t> s0;  // [32][16][2], steps0 rows used
   std::vector<uint16_t> s1; // [steps1][pairs1][2]
   unsigned long long version = 0ull;
-  std::string sdy, snp1;    // where other outer tables of the family come from (batched form)
+  std::string sdy, snp0, snp1; // where other tables of the families come from (batched and split forms)
 };
 
 std::mutex g_mtx;
@@ -700,6 +700,49 @@ int noalloc_sweeps(const unsigned routine, const unsigned nrow, const unsigned n
                          glb_b);
 }
 
+int family_tables(const unsigned n0, const unsigned n1, std::vector<uint8_t> &s0, unsigned &steps0,
+                  std::vector<uint16_t> &s1, unsigned &steps1, unsigned long long &version)
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  if (!g_strat.loaded)
+    return GJX_ERR_NO_STRAT;
+  if (!strat_id(g_strat.snp0.c_str(), n0, steps0) || !strat_id(g_strat.snp1.c_str(), n1, steps1)) {
+    g_err = "unknown strategy family";
+    return GJX_ERR_NO_STRAT;
+  }
+  void *const h = dlopen(g_strat.sdy.c_str(), RTLD_LAZY);
+  if (!h) {
+    g_err = "cannot open " + g_strat.sdy;
+    return GJX_ERR_NO_STRAT;
+  }
+  const void *const a0 = strat_ptr(h, g_strat.snp0.c_str(), n0);
+  const void *const a1 = strat_ptr(h, g_strat.snp1.c_str(), n1);
+  if (!a0 || !a1) {
+    dlclose(h);
+    g_err = "no " + (a0 ? g_strat.snp1 + " table for n = " + std::to_string(n1)
+                        : g_strat.snp0 + " table for n = " + std::to_string(n0)) + " in " + g_strat.sdy;
+    return GJX_ERR_NO_STRAT;
+  }
+  const size_t e0 = (size_t)steps0 * n0, e1 = (size_t)steps1 * n1; // steps x (n / 2 pairs) x 2
+  s0.resize(e0);
+  if (n0 <= 256u)
+    std::memcpy(s0.data(), a0, e0);
+  else { // the split form's inner tables are 64 columns; larger ones are refused by the caller
+    dlclose(h);
+    g_err = "inner table too large";
+    return GJX_ERR_NO_STRAT;
+  }
+  s1.resize(e1);
+  if (n1 <= 256u)
+    for (size_t i = 0u; i < e1; ++i)
+      s1[i] = static_cast<const uint8_t *>(a1)[i];
+  else
+    std::memcpy(s1.data(), a1, e1 * sizeof(uint16_t));
+  dlclose(h);
+  version = g_strat.version;
+  return 0;
+}
+
 int check_dev_args(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
                    const double *const dG, const unsigned lddG, const double *const dV, const unsigned lddV,
                    const double *const dD, const unsigned *const glbSwp, const unsigned long long *const glb_s,
@@ -779,6 +822,7 @@ int gjx_init_strats(const char *const sdy, const char *const snp0, const unsigne
     std::memcpy(s.s1.data(), a1, e1 * sizeof(uint16_t));
   dlclose(h);
   s.sdy = sdy;
+  s.snp0 = snp0;
   s.snp1 = snp1;
   s.loaded = true;
   std::lock_guard<std::mutex> lk(g_mtx);

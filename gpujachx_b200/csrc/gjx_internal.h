@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -109,6 +110,10 @@ int check_dev_args(unsigned routine, unsigned nrow, unsigned ncol, unsigned nplu
                    const double *dV, unsigned lddV, const double *dD, const unsigned *glbSwp,
                    const unsigned long long *glb_s, const unsigned long long *glb_b);
 void set_error(const char *msg);
+// the loaded strategy families' tables for n0 inner and n1 outer columns (the
+// split form: 64 and ncol / 32), as bytes and uint16; 0 or an error code
+int family_tables(unsigned n0, unsigned n1, std::vector<uint8_t> &s0, unsigned &steps0, std::vector<uint16_t> &s1,
+                  unsigned &steps1, unsigned long long &version);
 
 // exposed for the parity tests of the primitives
 cudaError_t launch_rsqrt_test(const double *in, double *out, unsigned n, cudaStream_t s);

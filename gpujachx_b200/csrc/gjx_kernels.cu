@@ -84,12 +84,6 @@ constexpr uint32_t kUpdBoxBytes = 34u * 8u * 16u * 8u;
 constexpr unsigned kRegion =
     (kGramStages * kGramStage > kUpdStages * kUpdStage) ? kGramStages * kGramStage : kUpdStages * kUpdStage;
 
-// one inner rotation, as the lanes that compute it hand it to those that apply it
-struct Rot {
-  double c, t, t_;
-  int mode; // 0 nothing, 1 rotate, 2 swap columns
-  int scale, swap;
-};
 
 // shared memory map (in doubles)
 constexpr unsigned kOffR = kRegion;        // R, 32x32 (later B^T, 32x34)
@@ -416,69 +410,6 @@ __device__ __forceinline__ void chol32_grp(double *const R, const unsigned gt, c
 // Every operation is the reference's (share/device_code_nosort.hpp:4-222,
 // share/device_code_cdsort.hpp:25-167, share/device_code_cdsort_KISS.hpp).
 // ---------------------------------------------------------------------------
-// rotT (trig) or rotH; when the two halves of the warp need different kinds,
-// both are computed and selected, so the warp does not run them one after
-// the other (each is a long dependent chain of divisions and square roots)
-__device__ __forceinline__ int rot_either(const bool trig, const double Apq, const double Dp, const double Dq,
-                                          double &c, double &t)
-{
-  if (__all_sync(0xffffffffu, trig))
-    return rotT(Apq, Dp, Dq, c, t);
-  if (__all_sync(0xffffffffu, !trig))
-    return rotH(Apq, Dp, Dq, c, t);
-  double c1, t1, c2, t2;
-  const int b1 = rotT(Apq, Dp, Dq, c1, t1), b2 = rotH(Apq, Dp, Dq, c2, t2);
-  c = trig ? c1 : c2;
-  t = trig ? t1 : t2;
-  return trig ? b1 : b2;
-}
-
-template <bool SORT>
-__device__ __forceinline__ Rot inner_rot(const double Dp, const double Dq, const double Apq, const unsigned p,
-                                         const unsigned q, const int definite, const unsigned npos, unsigned &ts_out,
-                                         unsigned &tb_out)
-{
-  // branch-free: the two half-warps handle different pairs, so every choice
-  // below is a select of values computed by both (no divergent paths)
-  Rot r;
-  const double Dp_ = __dsqrt_rn(Dp), Dq_ = __dsqrt_rn(Dq), Apq_ = fabs(Apq), Dpq_ = Dp_ * Dq_;
-  const int ts = !(Apq_ < (Dpq_ * kMyTol));
-  int tb;
-  if (!SORT) {
-    // the rotation is computed whether or not it is applied (no side
-    // effects), so that its latency overlaps the relative test
-    const bool trig = definite || ((p < npos) && (q < npos)) || ((p >= npos) && (q >= npos));
-    double c, t;
-    const int b = rot_either(trig, Apq, Dp, Dq, c, t);
-    r.c = ts ? c : 1.0;
-    r.t = ts ? t : 0.0;
-    r.t_ = ts ? (trig ? -t : t) : 0.0;
-    tb = ts ? b : 0;
-    r.mode = ts;
-    r.scale = tb;
-    r.swap = 0;
-  }
-  else {
-    const int def = definite ? definite : ((p < npos) && (q < npos)) ? +1 : ((p >= npos) && (q >= npos)) ? -1 : 0;
-    double c, t;
-    const int b = rot_either(def != 0, Apq, Dp, Dq, c, t);
-    const double t_ = def ? -t : t;
-    const double Dp2 = __fma_rn(t, Apq, Dp), Dq2 = __fma_rn(t_, Apq, Dq); // used when ts and def
-    const int swp = !((!def) || ((def > 0) && (Dp2 >= Dq2)) || ((def < 0) && (Dp2 <= Dq2)));
-    const int order = ((def > 0) && (Dp < Dq)) || ((def < 0) && (Dq < Dp));
-    r.c = ts ? c : 1.0;
-    r.t = ts ? t : 0.0;
-    r.t_ = ts ? t_ : 0.0;
-    tb = ts ? b : 0;
-    r.mode = ts ? 1 : (order ? 2 : 0);
-    r.scale = tb;
-    r.swap = ts ? swp : 0;
-  }
-  ts_out = (unsigned)ts;
-  tb_out = (unsigned)tb;
-  return r;
-}
-
 // apply rotation r to row x of columns p, q of R (values Gp, Gq, already
 // loaded) and of V_loc (Vp, Vq); mode 0 leaves them, 2 swaps the columns
 __device__ __forceinline__ void inner_apply(double *const R, double *const Vl, const unsigned p, const unsigned q,

@@ -205,6 +205,25 @@ int gjx_hypJacL2_noalloc(const unsigned routine, const unsigned nrow, const unsi
                          double *const dD, void *const stream, unsigned *const glbSwp,
                          unsigned long long *const glb_s, unsigned long long *const glb_b);
 
+/*
+ * Split-precision form (no counterpart in the reference, which has only the
+ * FP64 form): gjx_hypJacL2_dev's arguments and outputs, the same one-sided
+ * Jacobi with blocks of 32 columns and pairs of 64 (the loaded families'
+ * tables for n1 = ncol / 32 outer and 64 inner columns), the Gram matrix of
+ * each block pair and the update of G and V run as exact products of 8-bit
+ * slices on the tensor cores (tcgen05 kind::i8, int32 accumulators),
+ * recombined in FP64: 8 digits of 7 bits per entry, scaled per column by its
+ * largest entry, the slice products of digit weight above 2^-56 kept.  The
+ * Cholesky factors, rotations, convergence test and D stay FP64.  The
+ * results are not the plain form's bits; their accuracy is that of FP64
+ * arithmetic (tests report it against LAPACK and the plain form).  ncol a
+ * multiple of 64, nrow <= 61440; other codes as gjx_hypJacL2_dev.
+ */
+int gjx_hypJacL2_split(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
+                       double *const dG, const unsigned lddG, double *const dV, const unsigned lddV,
+                       double *const dD, void *const stream, unsigned *const glbSwp,
+                       unsigned long long *const glb_s, unsigned long long *const glb_b);
+
 /* Frees the device buffers that hypJacL2 keeps between calls on the current
  * device (they are reused by the next call of the same or smaller size). */
 int gjx_release_cache(void);
