@@ -595,6 +595,128 @@ def plain_loop_sample(Gs, Vs, Ds, G0, offs, sizes, nplus, per_size: int = 8):
             "sample": f"{per_size} matrices of each n through gjx_hypJacL2_dev, scaled to the batch"}
 
 
+def main_split(args):
+    """The split-precision form (gjx_hypJacL2_split) on a single-matrix
+    workload: device-resident value, e2e with the host copies, the roofline
+    of its update kernel (HBM-bound; the int8 tensor work per launch is given
+    beside it), accuracy against the FP64 reference spectrum and the plain
+    form's result on request (--accuracy)."""
+    import torch
+    import gpujachx_b200 as g
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    g.init_strats(None, "cycwor", 32, "cycwor", N1)
+    G0 = _input()
+    G0d = torch.tensor(np.ascontiguousarray(G0.T), dtype=torch.float64, device=dev)
+    dG = torch.empty_like(G0d)
+    full = bool(ALG & 2)
+    dV = torch.empty((N, N), dtype=torch.float64, device=dev)
+    dD = torch.empty(N, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        dG.copy_(G0d)
+        return g.hypJacL2_split(ALG, dG, NPLUS, dV, dD)[1]
+
+    for _ in range(args.warmup):
+        sweeps = step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    g.profile(True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sweeps = step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    prof = g.profile_read()
+    g.profile(False)
+    clk = clocks.stop()
+    value, total_ms = replica_throughput(sum(times), args.steps, world, dev)
+    pairs = N // 64
+    tiles = (M + 127) // 128 + ((N + 127) // 128 if full else 0)
+    upd_bytes = pairs * (M + (N if full else 0)) * 64 * 8 * 2       # each tile read and written once
+    upd_ops = pairs * tiles * 72 * 128 * 64 * 32 * 2                  # int8 multiply-adds x 2
+    upd_s = prof["l1_ms"] / max(1, prof["l1_launches"]) / 1000.0
+    hbm, peak_kind = _peaks()
+    steps1 = pairs * 2 - 1
+    fp64_flop = steps1 * pairs * (2 * M * 64 * 64 + 2 * (M + (N if full else 0)) * 64 * 64) * sweeps
+    roof = {"bound": "hbm", "achieved": upd_bytes / upd_s / 1e9, "peak": hbm, "unit": "GB/s",
+            "frac": upd_bytes / upd_s / 1e9 / hbm, "traffic": None,
+            "kernel": "gjx::split::sp_update_kernel<%s>" % ("true" if full else "false"),
+            "peak_kind": f"{peak_kind} HBM copy bandwidth", "per": "update launch (one per outer step), event time",
+            "launch_ms": upd_s * 1000.0, "launches": prof["l1_launches"],
+            "algorithmic_bytes_per_launch": upd_bytes, "int8_tensor_ops_per_launch": upd_ops,
+            "int8_tops": upd_ops / upd_s / 1e12,
+            "fp64_equivalent_tflops_whole_call": fp64_flop / (statistics.median(times) / 1000.0) / 1e12}
+    # e2e: pinned host input, H2D + the split call + D2H of U, V, D
+    hin = torch.empty((N, M), dtype=torch.float64, pin_memory=True)
+    hin.copy_(G0d)
+    hU = torch.empty_like(hin, pin_memory=True)
+    hV = torch.empty((N, N), dtype=torch.float64, pin_memory=True)
+    hD = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    e2e_t = []
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dG.copy_(hin, non_blocking=True)
+        g.hypJacL2_split(ALG, dG, NPLUS, dV, dD)
+        hU.copy_(dG, non_blocking=True)
+        if full:
+            hV.copy_(dV, non_blocking=True)
+        hD.copy_(dD, non_blocking=True)
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            e2e_t.append(time.perf_counter() - t0)
+    e2e_v, _ = replica_throughput(sum(e2e_t) * 1000.0, args.steps, world, dev)
+    e2e = {"value": e2e_v, "unit": "matrices/s", "h2d_bytes_per_step": M * N * 8,
+           "d2h_bytes_per_step": M * N * 8 + (N * N * 8 if full else 0) + N * 8,
+           "api": "gjx_hypJacL2_split (pinned host buffers, H2D and D2H around it)"}
+    line = {"metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (int8 slices on the tensor cores)",
+            "data": "synthetic",
+            "config": dict(CONFIG, form="split-precision (blocks of 32, pairs of 64, 8 int8 digits per entry)",
+                           parallelism=("replicas" if world > 1 else "single GPU")),
+            "sweeps": sweeps, "e2e": e2e, "roofline": roof, "clocks": clk, "gpu_launches": prof["launches"],
+            "step_ms": times}
+    if rank == 0 and args.accuracy:
+        line["accuracy"] = accuracy_figures(G0, dG.cpu().numpy().T, dV.cpu().numpy().T if full else None,
+                                            dD.cpu().numpy())
+        # the plain form on the same input, for the same figures
+        g.init_strats(None, "cycwor", 32, "cycwor", N1)
+        dG.copy_(G0d)
+        t0 = time.perf_counter()
+        _, sw_p, _, _ = g.hypJacL2_dev(ALG, dG, NPLUS, dV, dD)
+        torch.cuda.synchronize()
+        line["plain_form"] = {"seconds": time.perf_counter() - t0, "sweeps": sw_p,
+                              "accuracy": accuracy_figures(G0, dG.cpu().numpy().T,
+                                                           dV.cpu().numpy().T if full else None, dD.cpu().numpy())}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -606,12 +728,16 @@ def main():
     ap.add_argument("--accuracy", action="store_true", help="add pp80 figures of the last decomposition")
     ap.add_argument("--shard", action="store_true", help="c5 over N ranks: split one batch instead of N batches")
     ap.add_argument("--count", type=int, default=0, help="c5: matrices in the batch (default 4096; profiling runs)")
+    ap.add_argument("--form", default="plain", choices=["plain", "split"],
+                    help="plain FP64 (the drop-in) or the split-precision form (gjx_hypJacL2_split)")
     args = ap.parse_args()
     _use(args.config)
     if args.impl == "reference":
         return reference_arm(args)
     if args.config == "c5":
         return main_batch(args)
+    if args.form == "split":
+        return main_split(args)
 
     import torch
     import torch.distributed as dist

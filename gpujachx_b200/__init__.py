@@ -77,6 +77,8 @@ def lib() -> ctypes.CDLL:
     L.gjx_hypJacL2_noalloc.restype = i
     L.gjx_hypJacL2_split.argtypes = L.gjx_hypJacL2_dev.argtypes
     L.gjx_hypJacL2_split.restype = i
+    L.gjx_split_phase_cycles.argtypes = [ctypes.POINTER(ctypes.c_longlong)]
+    L.gjx_split_phase_cycles.restype = i
     L.gjx_release_cache.argtypes = []
     L.gjx_release_cache.restype = i
     L.gjx_set_verbose.argtypes = [i]

@@ -759,6 +759,20 @@ int check_dev_args(const unsigned routine, const unsigned nrow, const unsigned n
 
 void set_error(const char *msg) { g_err = msg; }
 
+bool profiling()
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  return g_prof.on;
+}
+
+void profile_add(const unsigned long long launches, const unsigned long long timed, const double ms)
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  g_prof.launches += launches;
+  g_prof.l1_launches += timed;
+  g_prof.l1_ms += ms;
+}
+
 } // namespace gjx
 
 extern "C" {

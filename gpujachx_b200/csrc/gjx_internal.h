@@ -110,6 +110,10 @@ int check_dev_args(unsigned routine, unsigned nrow, unsigned ncol, unsigned nplu
                    const double *dV, unsigned lddV, const double *dD, const unsigned *glbSwp,
                    const unsigned long long *glb_s, const unsigned long long *glb_b);
 void set_error(const char *msg);
+// the profiling counters of gjx_profile: whether launches are timed, and
+// launches / timed launches / their milliseconds to add
+bool profiling();
+void profile_add(unsigned long long launches, unsigned long long timed, double ms);
 // the loaded strategy families' tables for n0 inner and n1 outer columns (the
 // split form: 64 and ncol / 32), as bytes and uint16; 0 or an error code
 int family_tables(unsigned n0, unsigned n1, std::vector<uint8_t> &s0, unsigned &steps0, std::vector<uint16_t> &s1,

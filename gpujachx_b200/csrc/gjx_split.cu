@@ -17,19 +17,24 @@
 //
 // Slicing (Ozaki's scheme, balanced digits).  A column c of the operand is
 // scaled by 2^-e_c, e_c the exponent bound of its largest |entry| (|a| <
-// 2^e_c), so each entry becomes x = a 2^-e_c in (-1, 1); v = rint(x 2^55) is a
-// 56-bit integer, written as v = sum_t d_t 2^(49 - 7t), t = 0..7: d_0 in
-// [-64, 64], d_1..d_7 in [-64, 63] (balanced base-128 digits).  Each digit
-// plane is an int8 matrix.  A product of two such operands is
-//   sum_k v_ik w_kj = sum_(t,u) 2^(98 - 7(t+u)) sum_k d_t,ik d_u,kj,
-// and the slice products with t + u <= 7 are kept: 36 int8 x int8 -> int32
-// products, summed exactly per group g = t + u in 8 int32 accumulators, then
-// F = sum_g 2^-7g S_g in FP64 (Horner, low groups first) and a power-of-two
-// scale.  The slicing error is 2^-56 of the column's scale per entry, the
-// truncation of the groups g >= 8 about 2^-55 of the product's scale: the
-// order of FP64 rounding.  The scales are tracked exactly: the update kernel
-// folds the largest |entry| of every column it writes into a per-column word
-// (atomic max of the high words), read by the next step (by step parity).
+// 2^e_c), so each entry becomes x = a 2^-e_c in (-1, 1); v = rint(x 2^54) is a
+// 55-bit integer, written as v = sum_t d_t 2^(8 (6 - t)), t = 0..6: d_0 in
+// [-64, 65], d_1..d_6 in [-128, 127] (balanced base-256 digits: with 128
+// added to each of the six low bytes of v, digit t is byte 6 - t of the sum
+// with its top bit flipped, so cutting a value is a handful of byte
+// permutes).  Each digit plane is an int8 matrix.  A product of two such
+// operands is
+//   sum_k v_ik w_kj = sum_(t,u) 2^(96 - 8(t+u)) sum_k d_t,ik d_u,kj,
+// and the slice products with t + u <= 6 are kept: 28 int8 x int8 -> int32
+// products, summed exactly per group g = t + u in 7 int32 accumulators, then
+// combined in int64 (groups 0-3 and 4-6), two conversions, one FMA and a
+// power-of-two scale.  The slicing error is 2^-55 of the column's scale per
+// entry, the dropped groups g >= 7 weigh about 2^-56 of the product's scale:
+// the order of FP64 rounding.  The scales are tracked exactly: the update
+// kernel folds the largest |entry| of every column it writes into a
+// per-column word (atomic max of the high words), read by the next step (by
+// step parity).  The int32 group sums bound the Gram's rows: 7 x 2^14 x nrow
+// < 2^31, nrow <= 16384.
 //
 // Kernels, per outer step:
 //   sp_pair_kernel    one CTA per block pair: the Gram matrix (TMA tensor
@@ -40,10 +45,10 @@
 //                     inner sweep(s), and the digit planes of the update's B
 //                     operand diag(2^e) V_loc (for G and for V) in global
 //                     memory;
-//   sp_update_kernel  one CTA per 128 rows of a pair's columns of G or V: the
-//                     FP64 tile by TMA, sliced, 72 MMAs of 128 x 64 x 32, the
-//                     epilogue back to FP64 in place by TMA stores, and the
-//                     tile's column maxima.
+//   sp_update_kernel  a persistent grid over the 128-row tiles of every pair's
+//                     columns of G and V: the FP64 tile by TMA (two ahead),
+//                     sliced, 72 MMAs of 128 x 64 x 32, the epilogue back to
+//                     FP64 in place, and the columns' maxima.
 // Every wait is bounded (kWait cycles): on a timeout the kernel sets the
 // error word and leaves.
 #include <cudaTypedefs.h>
@@ -61,13 +66,13 @@ namespace split {
 constexpr unsigned kThreads = 256u;
 constexpr unsigned kBW = 32u;    // columns per block
 constexpr unsigned kW = 64u;     // columns per block pair
-constexpr unsigned kDig = 8u;    // digits per value
+constexpr unsigned kDig = 7u;    // digits per value
 constexpr long long kWait = 2000000000ll;
 constexpr unsigned kTmemCols = 512u; // 8 accumulators x 64 columns
-// sum_{t=1..7} 64 * 2^(49 - 7t): added before cutting the low digits so that
-// each becomes a field in [0, 127] standing for the digit + 64
-constexpr long long kDigitBias = 64ll * ((1ll << 42) + (1ll << 35) + (1ll << 28) + (1ll << 21) + (1ll << 14) +
-                                         (1ll << 7) + 1ll);
+// 128 in each of the six low bytes: added to v so that each low byte holds
+// its digit + 128
+constexpr long long kDigitBias = 128ll * 0x010101010101ll;
+constexpr unsigned kMaxRows = 16384u; // int32 group sums of the Gram matrix: 7 x 2^14 x nrow < 2^31
 
 struct Params {
   CUtensorMap tmGram; // 3-D view (64 rows, tiles, columns) of G, box {66, 1, 16} (the plain form's)
@@ -80,10 +85,14 @@ struct Params {
   uint32_t *cmaxG; // [2][ncol]: high word of the largest |entry| of each column, by step parity
   uint32_t *cmaxV; // [2][ncol]
   uint8_t *bop;    // per pair: the update's B operands (G, then V): kBopBytes each
+  double *G, *V;
+  unsigned ldG, ldV;
   unsigned nrow, ncol, nplus, pairs, step, parity, s0steps, nswp0;
   unsigned tilesG, tilesV; // 128-row tiles of G and of V
   int gdefinite;
   int accv;
+  unsigned sms; // CTAs of the persistent update grid
+  long long *clk; // block 0 of sp_pair_kernel: clock64 at the phase ends (gjx_split_phase_cycles)
 };
 
 // ---- the update's B operand in global memory: 8 digit planes (K-major,
@@ -180,8 +189,9 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap *tm, const void *
 // digits
 // ---------------------------------------------------------------------------
 // exponent bound of a column from the high word of its largest |entry|:
-// every entry is below 2^e (a zero or subnormal column: e = -1022)
-__device__ __forceinline__ int col_exp(const uint32_t hw) { return (int)((hw >> 20) & 0x7FFu) - 1022; }
+// every entry is below 2^e; columns below 2^-969 (zero ones among them) are
+// given e = -969, so that 2^(54 - e) and its inverse stay normal
+__device__ __forceinline__ int col_exp(const uint32_t hw) { return max((int)((hw >> 20) & 0x7FFu) - 1022, -969); }
 
 // 2^k for k in [-1022, 1023]
 __device__ __forceinline__ double p2(const int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
@@ -194,60 +204,50 @@ __device__ __forceinline__ double scale2(const double x, const int k)
   return (x * p2(k1)) * p2(k - k1);
 }
 
-// the 56-bit integer of a * 2^(55 - e) (|a| < 2^e), biased for digit cutting
-__device__ __forceinline__ long long biased_int(const double a, const int e)
+// 2^(54 - e) for a column with exponent bound e
+__device__ __forceinline__ double cut_factor(const int e) { return p2(54 - e); }
+
+// the 55-bit integer of a * f (f = cut_factor(e), |a| < 2^e: |a f| < 2^54),
+// biased for digit cutting
+__device__ __forceinline__ long long biased_int(const double a, const double f)
 {
-  long long v = __double2ll_rn(scale2(a, 55 - e));
-  v = max(min(v, 1ll << 55), -(1ll << 55)); // |a| < 2^e holds by construction; never exceed the digit range
-  return v + kDigitBias;
+  return __double2ll_rn(a * f) + kDigitBias;
 }
 
-// plane t's bytes of four values (the words w[0..3] from biased_int): byte j
-// of the result is digit t of value j as an int8
-template <unsigned T> __device__ __forceinline__ uint32_t plane_word(const long long (&w)[4])
+// plane T's bytes of four biased values: byte j of the result is digit T of
+// value j as an int8 (byte 6 - T of the value; the low digits' top bits flipped)
+template <unsigned T> __device__ __forceinline__ uint32_t plane_word(const long long w0, const long long w1,
+                                                                     const long long w2, const long long w3)
 {
-  if (T == 0u) { // d_0 = w >> 49 in [-64, 64]: its 8 low bits
-    uint32_t r = 0u;
-#pragma unroll
-    for (unsigned j = 0u; j < 4u; ++j)
-      r |= ((uint32_t)(w[j] >> 49) & 0xFFu) << (8u * j);
-    return r;
-  }
-  else { // field f = bits [49 - 7T, 56 - 7T) in [0, 127] stands for f - 64: sign-extend (f ^ 64) from 7 bits
-    uint32_t r = 0u;
-#pragma unroll
-    for (unsigned j = 0u; j < 4u; ++j)
-      r |= ((uint32_t)(w[j] >> (49u - 7u * T)) & 0x7Fu) << (8u * j);
-    r ^= 0x40404040u;
-    return r | ((r & 0x40404040u) << 1);
-  }
+  constexpr unsigned B = 6u - T;             // byte of the value
+  constexpr unsigned sel = (B & 3u) | ((4u + (B & 3u)) << 4); // bytes B of x and of y, to bytes 0 and 1
+  const uint32_t x0 = (B >= 4u) ? (uint32_t)((unsigned long long)w0 >> 32) : (uint32_t)w0;
+  const uint32_t x1 = (B >= 4u) ? (uint32_t)((unsigned long long)w1 >> 32) : (uint32_t)w1;
+  const uint32_t x2 = (B >= 4u) ? (uint32_t)((unsigned long long)w2 >> 32) : (uint32_t)w2;
+  const uint32_t x3 = (B >= 4u) ? (uint32_t)((unsigned long long)w3 >> 32) : (uint32_t)w3;
+  const uint32_t lo = __byte_perm(x0, x1, sel), hi = __byte_perm(x2, x3, sel);
+  const uint32_t r = __byte_perm(lo, hi, 0x5410u);
+  return (T == 0u) ? r : (r ^ 0x80808080u);
 }
 
-// 16 values -> 16 bytes of each of the 8 planes
+// 16 biased values -> 16 bytes of each of the 7 planes
 __device__ __forceinline__ void digits16(const long long (&w)[16], uint4 (&out)[kDig])
 {
 #define GJX_PLANE(T)                                                                                                 \
-  {                                                                                                                  \
-    uint32_t q[4];                                                                                                   \
-    _Pragma("unroll") for (unsigned k = 0u; k < 4u; ++k)                                                             \
-    {                                                                                                                \
-      const long long ww[4] = {w[4u * k], w[4u * k + 1u], w[4u * k + 2u], w[4u * k + 3u]};                           \
-      q[k] = plane_word<T>(ww);                                                                                      \
-    }                                                                                                                \
-    out[T] = make_uint4(q[0], q[1], q[2], q[3]);                                                                     \
-  }
-  GJX_PLANE(0u) GJX_PLANE(1u) GJX_PLANE(2u) GJX_PLANE(3u) GJX_PLANE(4u) GJX_PLANE(5u) GJX_PLANE(6u) GJX_PLANE(7u)
+  out[T] = make_uint4(plane_word<T>(w[0], w[1], w[2], w[3]), plane_word<T>(w[4], w[5], w[6], w[7]),                \
+                      plane_word<T>(w[8], w[9], w[10], w[11]), plane_word<T>(w[12], w[13], w[14], w[15]));
+  GJX_PLANE(0u) GJX_PLANE(1u) GJX_PLANE(2u) GJX_PLANE(3u) GJX_PLANE(4u) GJX_PLANE(5u) GJX_PLANE(6u)
 #undef GJX_PLANE
 }
 
-// F = sum_g 2^-7g S_g, low groups first
-__device__ __forceinline__ double recombine(const int (&s)[kDig])
+// sum_g 2^-8g S_g, times 2^24: groups 0-3 and 4-6 each summed exactly in
+// int64, then two conversions and one FMA
+__device__ __forceinline__ double recombine(const int s0, const int s1, const int s2, const int s3, const int s4,
+                                           const int s5, const int s6)
 {
-  double f = (double)s[7];
-#pragma unroll
-  for (int g = 6; g >= 0; --g)
-    f = __fma_rn(f, 0x1.0p-7, (double)s[g]);
-  return f;
+  const long long H = ((long long)s0 << 24) + ((long long)s1 << 16) + ((long long)s2 << 8) + (long long)s3;
+  const long long L = ((long long)s4 << 16) + ((long long)s5 << 8) + (long long)s6;
+  return __fma_rn(__ll2double_rn(L), 0x1.0p-24, __ll2double_rn(H));
 }
 
 __device__ __forceinline__ uint32_t abs_hi(const double x)
@@ -264,23 +264,24 @@ __device__ __forceinline__ uint32_t abs_hi(const double x)
 constexpr unsigned kGStages = 3u;
 constexpr uint32_t kGBox = 66u * 16u * 8u;         // 8448 bytes
 constexpr uint32_t kGStageBytes = 4u * kGBox;       // 33792
-// digit planes of a 64-row tile: 2 chunks of 32 rows x 8 planes x 2 KB; the
-// planes of a chunk in the order 0, 4, 1, 5, 2, 6, 3, 7 so that planes t and
-// t + 4 form one 128-row A operand
+// digit planes of a 64-row tile: 2 chunks of 32 rows x 8 plane slots x 2 KB
+// (K-major: 64 columns x 32 rows; slot 7 is never written).  The planes of a
+// chunk lie in digit order, so planes t, t + 1 form one 128-row A operand and
+// planes u .. u + 3 one 256-column B operand.
 constexpr uint32_t kGPlane = 2048u;
-constexpr uint32_t kGChunk = kDig * kGPlane;        // 16384
+constexpr uint32_t kGChunk = 8u * kGPlane;          // 16384
 constexpr uint32_t kGTilePlanes = 2u * kGChunk;     // 32768
 constexpr unsigned kGPlaneBufs = 2u;
 constexpr uint32_t kOffGStage = 0u;
 constexpr uint32_t kOffGPlanes = kGStages * kGStageBytes;                     // 101376
 constexpr uint32_t kOffGEnd = kOffGPlanes + kGPlaneBufs * kGTilePlanes;       // 166912
 // after the Gram (reusing the staging): R and V_loc (64 x 64, ld 65), the
-// groups 4..7 of the bottom accumulator halves (int32 [4][64][64])
+// bottom halves of accumulator blocks 0..5 (int32 [6][64][64]: groups 1..6)
 constexpr unsigned kLd = 65u;
 constexpr uint32_t kOffR = 0u;
 constexpr uint32_t kOffVl = kOffR + 64u * kLd * 8u;                          // 33280
-constexpr uint32_t kOffBot = kOffVl + 64u * kLd * 8u;                        // 66560, 65536 bytes
-static_assert(kOffBot + 65536u <= kOffGEnd, "Gram epilogue scratch must fit");
+constexpr uint32_t kOffBot = kOffVl + 64u * kLd * 8u;                        // 66560, 98304 bytes
+static_assert(kOffBot + 6u * 64u * 64u * 4u <= kOffGEnd, "Gram epilogue scratch must fit");
 // fixed region after it
 constexpr uint32_t kOffS0 = kOffGEnd;                                        // inner table, 64 steps x 64 bytes
 constexpr uint32_t kOffScale = kOffS0 + 4096u;                               // 64 int: e_c of G; 64 int: of V
@@ -473,10 +474,11 @@ __device__ void bop_write(const double *const Vl, const int *const e, uint8_t *c
   hw = max(hw, __shfl_xor_sync(0xffffffffu, hw, 1));
   hw = max(hw, __shfl_xor_sync(0xffffffffu, hw, 2));
   const int h = col_exp(hw);
+  const double f = cut_factor(h);
   long long w[16];
 #pragma unroll
   for (unsigned i = 0u; i < 16u; ++i)
-    w[i] = biased_int(b[i], h);
+    w[i] = biased_int(b[i], f);
   uint4 pl[kDig];
   digits16(w, pl);
 #pragma unroll
@@ -503,6 +505,10 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
   const unsigned ntiles = (P.nrow + 63u) / 64u;
   __shared__ int s_fail;
 
+  const bool rec = pair == 0u && tid == 0u;
+  long long t_start = 0;
+  if (rec)
+    t_start = clock64();
   if (tid == 0u) {
     s_fail = 0;
     for (unsigned i = 0u; i < 5u; ++i)
@@ -537,8 +543,7 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
   }
   // slicing task of this thread: column x, rows 16 rg .. 16 rg + 15 of the tile
   const unsigned x = tid & 63u, rg = tid >> 6;
-  const int ex = eG[x];
-  constexpr uint32_t kId = idesc_i8(128u, 64u);
+  const double fx = cut_factor(eG[x]);
   for (unsigned i = 0u; i < ntiles; ++i) {
     const unsigned s = i % kGStages, b = i & 1u;
     int bad = !mbar_wait_bounded(&bar[s], (i / kGStages) & 1u, kWait);
@@ -555,18 +560,16 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
 #pragma unroll
       for (unsigned k = 0u; k < 8u; ++k) {
         const double2 v = *reinterpret_cast<const double2 *>(col + 16u * rg + 2u * k);
-        w[2u * k] = biased_int(v.x, ex);
-        w[2u * k + 1u] = biased_int(v.y, ex);
+        w[2u * k] = biased_int(v.x, fx);
+        w[2u * k + 1u] = biased_int(v.y, fx);
       }
       uint4 pl[kDig];
       digits16(w, pl);
       uint8_t *const dst = sm + kOffGPlanes + b * kGTilePlanes + (rg >> 1) * kGChunk + (x >> 3) * 256u +
                            (rg & 1u) * 128u + (x & 7u) * 16u;
 #pragma unroll
-      for (unsigned t = 0u; t < kDig; ++t) {
-        const unsigned slot = (t < 4u) ? 2u * t : 2u * (t - 4u) + 1u;
-        *reinterpret_cast<uint4 *>(dst + slot * kGPlane) = pl[t];
-      }
+      for (unsigned t = 0u; t < kDig; ++t)
+        *reinterpret_cast<uint4 *>(dst + t * kGPlane) = pl[t];
     }
     fence_async_shared();
     __syncthreads();
@@ -582,19 +585,27 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
         tma_load_3d(dst + 3u * kGBox, &P.tmGram, 0, tile, (int)(jBlk * kBW + 16u), &bar[s]);
       }
       tc_fence_after();
-#pragma unroll 1
+      // A = planes 2p (rows 0-63) and 2p + 1 (rows 64-127; for p = 3 the
+      // unused slot 7), B = planes u0 .. u0 + n - 1 side by side: D block
+      // 2p + u0 + i gets group 2p + u0 + i in its top rows and group
+      // 2p + u0 + i + 1 in its bottom rows.  Every (t, u) with t + u <= 6 is
+      // covered; what lands in groups >= 7 is never read.
+      const uint64_t d0 = sdesc(sbase + kOffGPlanes + b * kGTilePlanes, 128u, 256u);
+      const uint32_t first = (i == 0u) ? 0u : 1u;
+#pragma unroll
       for (unsigned kc = 0u; kc < 2u; ++kc) {
-        const uint32_t base = sbase + kOffGPlanes + b * kGTilePlanes + kc * kGChunk;
-#pragma unroll 1
-        for (unsigned t = 0u; t < 4u; ++t) {
-          const uint64_t a = sdesc(base + 2u * t * kGPlane, 128u, 256u);
-#pragma unroll 1
-          for (unsigned u = 0u; u + t < kDig; ++u) {
-            const unsigned slot = (u < 4u) ? 2u * u : 2u * (u - 4u) + 1u;
-            const uint64_t bd = sdesc(base + slot * kGPlane, 128u, 256u);
-            mma_i8(tmem + (t + u) * 64u, a, bd, kId, (i == 0u && kc == 0u && t == 0u) ? 0u : 1u);
-          }
-        }
+        const uint64_t dc = d0 + ((kc * kGChunk) >> 4);
+        const uint32_t acc0 = (kc == 0u) ? first : 1u;
+#define GJX_GMMA(P, U0, NN, ACC)                                                                                     \
+  mma_i8(tmem + (2u * (P) + (U0)) * 64u, dc + ((2u * (P) * kGPlane) >> 4), dc + (((U0) * kGPlane) >> 4),             \
+         idesc_i8(128u, (NN) * 64u), (ACC))
+        GJX_GMMA(0u, 0u, 4u, acc0);
+        GJX_GMMA(0u, 4u, 3u, acc0);
+        GJX_GMMA(1u, 0u, 4u, 1u);
+        GJX_GMMA(1u, 4u, 1u, 1u);
+        GJX_GMMA(2u, 0u, 3u, 1u);
+        GJX_GMMA(3u, 0u, 1u, 1u);
+#undef GJX_GMMA
       }
       mma_commit(&bar[3u + b]);
     }
@@ -608,10 +619,13 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
   }
   const bool failed = __syncthreads_or(bad) != 0;
   tc_fence_after();
+  if (rec)
+    P.clk[0] = clock64() - t_start;
 
-  // Gram epilogue: warps 2, 3, 6, 7 (TMEM lanes 64..127: the planes t + 4)
-  // park their groups 4..7 in shared memory; warps 0, 1, 4, 5 add them to
-  // their groups and form the FP64 Gram entries (x = row, y = column)
+  // Gram epilogue: warps 2, 3, 6, 7 (TMEM lanes 64..127: the odd planes)
+  // park blocks 0..5 (groups 1..6) in shared memory; warps 0, 1, 4, 5 add
+  // them to their blocks' groups and form the FP64 Gram entries (x = row,
+  // y = column)
   double *const R = reinterpret_cast<double *>(sm + kOffR);
   double *const Vl = reinterpret_cast<double *>(sm + kOffVl);
   int *const bot = reinterpret_cast<int *>(sm + kOffBot);
@@ -619,7 +633,7 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
   if (!failed && q4 >= 2u) {
     const unsigned xr = (q4 - 2u) * 32u + lane;
 #pragma unroll 1
-    for (unsigned g = 0u; g < 4u; ++g)
+    for (unsigned g = 0u; g < 6u; ++g)
 #pragma unroll 1
       for (unsigned ch = 0u; ch < 2u; ++ch) {
         int v[16];
@@ -645,10 +659,11 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
       for (unsigned k = 0u; k < 16u; ++k) {
         const unsigned y = half * 32u + ch * 16u + k;
         int sg[kDig];
+        sg[0] = acc[0][k];
 #pragma unroll
-        for (unsigned g = 0u; g < kDig; ++g)
-          sg[g] = acc[g][k] + ((g >= 4u) ? bot[((g - 4u) * 64u + y) * 64u + xr] : 0);
-        R[y * kLd + xr] = scale2(recombine(sg), eG[xr] + eG[y] - 12);
+        for (unsigned g = 1u; g < kDig; ++g)
+          sg[g] = acc[g][k] + bot[((g - 1u) * 64u + y) * 64u + xr];
+        R[y * kLd + xr] = scale2(recombine(sg[0], sg[1], sg[2], sg[3], sg[4], sg[5], sg[6]), eG[xr] + eG[y] - 36);
       }
     }
   }
@@ -661,31 +676,57 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
       set_err(P);
     return;
   }
+  if (rec)
+    P.clk[1] = clock64() - t_start;
 
-  // Cholesky of the Gram matrix (lower triangle, in place): column k of L,
-  // then the trailing update, two barriers per column.  A pivot that is not
-  // positive (a column dependent on the previous ones to working accuracy)
-  // gives a zero column of L.
-  __shared__ double s_inv;
-  for (unsigned k = 0u; k < 64u; ++k) {
-    if (tid == 0u) {
-      const double d = R[k * kLd + k];
-      const double piv = d > 0.0 ? __dsqrt_rn(d) : 0.0;
-      R[k * kLd + k] = piv;
-      s_inv = piv > 0.0 ? __drcp_rn(piv) : 0.0;
+  // Cholesky of the Gram matrix (lower triangle, in place), one barrier per
+  // column: in round k warp 0 updates column k + 1 by column k and pivots it
+  // (L(i, j) = A(i, j) / sqrt(A(j, j)), by the reciprocal), while warps 1..7
+  // update columns k + 2 .. 63 by column k.  A pivot that is not positive (a
+  // column dependent on the previous ones to working accuracy) gives a zero
+  // column of L.  Lane x holds rows x and x + 32.
+  {
+    const auto pivot = [&](const unsigned j) {
+      __syncwarp();
+      const double d = R[j * kLd + j];
+      const double piv = d > 0.0 ? __dsqrt_rn(d) : 0.0, inv = piv > 0.0 ? __drcp_rn(piv) : 0.0;
+      __syncwarp();
+#pragma unroll
+      for (unsigned h = 0u; h < 2u; ++h) {
+        const unsigned i = lane + 32u * h;
+        if (i > j)
+          R[j * kLd + i] *= inv;
+        else if (i == j)
+          R[j * kLd + j] = piv;
+      }
+    };
+    if (warp == 0u)
+      pivot(0u);
+    __syncthreads();
+    for (unsigned k = 0u; k + 1u < 64u; ++k) {
+      if (warp == 0u) {
+        const unsigned j = k + 1u;
+        const double ljk = R[k * kLd + j];
+#pragma unroll
+        for (unsigned h = 0u; h < 2u; ++h) {
+          const unsigned i = lane + 32u * h;
+          if (i >= j)
+            R[j * kLd + i] = __fma_rn(-R[k * kLd + i], ljk, R[j * kLd + i]);
+        }
+        pivot(j);
+      }
+      else {
+        const double l0 = R[k * kLd + lane], l1 = R[k * kLd + lane + 32u];
+        for (unsigned j = k + 1u + warp; j < 64u; j += 7u) {
+          const double ljk = R[k * kLd + j];
+          if (lane >= j)
+            R[j * kLd + lane] = __fma_rn(-l0, ljk, R[j * kLd + lane]);
+          if (lane + 32u >= j)
+            R[j * kLd + lane + 32u] = __fma_rn(-l1, ljk, R[j * kLd + lane + 32u]);
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
-    const double inv = s_inv;
-    if (tid > k && tid < 64u)
-      R[k * kLd + tid] *= inv;
-    __syncthreads();
-    // A(i, j) -= L(i, k) L(j, k), k < j <= i
-    for (unsigned e = tid; e < 64u * 64u; e += kThreads) {
-      const unsigned i = e & 63u, j = e >> 6;
-      if (j > k && i >= j)
-        R[j * kLd + i] = __fma_rn(-R[k * kLd + i], R[k * kLd + j], R[j * kLd + i]);
-    }
-    __syncthreads();
   }
   // R = L^T (upper), V_loc = I
   for (unsigned e = tid; e < 64u * 64u; e += kThreads) {
@@ -706,11 +747,15 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
   }
   __syncthreads();
 
+  if (rec)
+    P.clk[2] = clock64() - t_start;
   int definite;
   unsigned npos;
   pair_signature(P, iBlk, jBlk, definite, npos);
   unsigned blk_s = 0u, blk_b = 0u;
   inner64<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, blk_s, blk_b);
+  if (rec)
+    P.clk[3] = clock64() - t_start;
 
   // the update's B operands, the counters, and the next step's column maxima cleared
   uint8_t *const bop = P.bop + (size_t)pair * (ACCV ? 2u : 1u) * kBopBytes;
@@ -729,51 +774,101 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
     else
       atomicAdd(reinterpret_cast<unsigned *>(P.cvg), blk_s);
   }
+  if (rec)
+    P.clk[4] = clock64() - t_start;
 }
 
 // ---------------------------------------------------------------------------
-// sp_update_kernel: C = A B for one 128-row tile of a pair's 64 columns of G
-// (tiles 0 .. tilesG - 1) or of V (the rest), A the FP64 tile, B = V_loc
-// (its digit planes diag(2^e) V_loc from sp_pair_kernel).  C replaces A.
+// sp_update_kernel: C = A B for 128-row tiles of the pairs' 64 columns of G
+// and V, A the FP64 tile, B = V_loc (its digit planes diag(2^e) V_loc from
+// sp_pair_kernel); C replaces A.  A persistent grid: CTA c takes a
+// contiguous run of the items (pair, tile), tiles of a pair in order (G's,
+// then V's), so its B operand changes rarely.  Per item: the FP64 tile
+// (TMA, two items ahead, double-buffered) is cut into the 8 digit planes of
+// A, 72 MMAs of 128 x 64 x 32 into 8 int32 accumulators, then each thread
+// recombines its row's outputs (int64 group sums, two conversions) and
+// stores them straight to global memory (a warp writes 256 contiguous bytes
+// per column), folding their magnitudes into the columns' maxima.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kUStage = 128u * 64u * 8u;     // FP64 tile, column c at c * 128 doubles
-constexpr uint32_t kUAPlane = 8192u;               // 128 x 64 bytes, K-major, LBO 128, SBO 512
-constexpr uint32_t kOffUStage = 0u;
-constexpr uint32_t kOffUA = kUStage;                            // 65536
-constexpr uint32_t kOffUB = kOffUA + kDig * kUAPlane;           // 131072
-constexpr uint32_t kOffUScale = kOffUB + kBopBytes;             // 163840 + 256: 64 int e_k, then 64 uint col max
-constexpr uint32_t kOffUBar = kOffUScale + 512u;
+constexpr uint32_t kUStage = 128u * 64u * 8u;                  // FP64 tile, column c at c * 128 doubles
+constexpr uint32_t kUAPlane = 8192u;                            // 128 x 64 bytes, K-major, LBO 128, SBO 512
+constexpr uint32_t kOffUStage = 0u;                             // two tiles
+constexpr uint32_t kOffUA = 2u * kUStage;                       // 131072
+constexpr uint32_t kOffUB = kOffUA + kDig * kUAPlane;           // 188416
+constexpr uint32_t kOffUScale = kOffUB + kBopBytes;             // 64 double cut factors, 64 double output
+                                                                // scales, [4][64] uint maxima of the row quarters
+constexpr uint32_t kOffUBar = kOffUScale + 2048u;               // [0, 1] tiles, [2] B operand, [3] MMAs
 constexpr uint32_t kOffUTmem = kOffUBar + 32u;
 constexpr uint32_t kUpdSmem = kOffUTmem + 16u;
 static_assert(kUpdSmem <= 227u * 1024u, "shared memory of sp_update_kernel");
+
+// int64 t (|t| < 2^51) as a double, exactly: the bits of 1.5 * 2^52 + t minus 1.5 * 2^52
+__device__ __forceinline__ double exact_ll(const long long t)
+{
+  return __longlong_as_double(t + 0x4338000000000000ll) - 0x1.8p+52;
+}
+
+// sum_g 2^-8g S_g (g = 0..6) in FP64: T0 = S0 2^8 + S1, T1 = S2 2^8 + S3,
+// T2 = S4 2^16 + S5 2^8 + S6 are exact int64 (below 2^48) and convert exactly;
+// two roundings
+__device__ __forceinline__ double recombine_u(const int s0, const int s1, const int s2, const int s3, const int s4,
+                                             const int s5, const int s6)
+{
+  const long long t0 = (long long)s0 * 256ll + (long long)s1;
+  const long long t1 = (long long)s2 * 256ll + (long long)s3;
+  const long long t2 = (long long)s4 * 65536ll + (long long)s5 * 256ll + (long long)s6;
+  return __fma_rn(exact_ll(t0), 0x1.0p-8, __fma_rn(exact_ll(t1), 0x1.0p-24, exact_ll(t2) * 0x1.0p-48));
+}
+
+struct Item {
+  unsigned pair, iBlk, jBlk, row0, rows, key;
+  bool isV;
+};
+
+__device__ __forceinline__ Item item_of(const Params &P, const unsigned k)
+{
+  const unsigned tiles = P.tilesG + P.tilesV;
+  Item it;
+  it.pair = k / tiles;
+  const unsigned t = k - it.pair * tiles;
+  it.isV = t >= P.tilesG;
+  it.row0 = (it.isV ? t - P.tilesG : t) * 128u;
+  it.rows = it.isV ? P.ncol : P.nrow;
+  it.key = 2u * it.pair + (it.isV ? 1u : 0u);
+  const uint16_t *const blk = P.strat1 + ((size_t)P.step * P.pairs + it.pair) * 2u;
+  it.iBlk = blk[0];
+  it.jBlk = blk[1];
+  return it;
+}
+
+__device__ __forceinline__ void load_tile(const Params &P, const Item &it, unsigned char *const dst, uint64_t *bar)
+{
+  const CUtensorMap *const tm = it.isV ? &P.tmV : &P.tmG;
+  mbar_arrive_expect_tx(bar, kUStage);
+  tma_load_2d(dst, tm, (int)it.row0, (int)(it.iBlk * kBW), bar);
+  tma_load_2d(dst + kUStage / 2u, tm, (int)it.row0, (int)(it.jBlk * kBW), bar);
+}
 
 template <bool ACCV>
 __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_constant__ Params P)
 {
   extern __shared__ __align__(1024) unsigned char sm[];
   const unsigned tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
-  const unsigned pair = blockIdx.y, tile = blockIdx.x;
-  const bool isV = tile >= P.tilesG;
-  const unsigned row0 = (isV ? tile - P.tilesG : tile) * 128u;
-  const uint16_t *const blk = P.strat1 + ((size_t)P.step * P.pairs + pair) * 2u;
-  const unsigned iBlk = blk[0], jBlk = blk[1];
-  const CUtensorMap *const tm = isV ? &P.tmV : &P.tmG;
-  uint32_t *const cmax = isV ? P.cmaxV : P.cmaxG;
-  uint64_t *const bar = reinterpret_cast<uint64_t *>(sm + kOffUBar); // [0] loads, [1] MMAs
+  const unsigned nitems = P.pairs * (P.tilesG + P.tilesV);
+  const unsigned per = nitems / gridDim.x, extra = nitems % gridDim.x;
+  const unsigned it0 = blockIdx.x * per + min(blockIdx.x, extra);
+  const unsigned it1 = it0 + per + (blockIdx.x < extra ? 1u : 0u);
+  uint64_t *const bar = reinterpret_cast<uint64_t *>(sm + kOffUBar);
   uint32_t *const tmem_holder = reinterpret_cast<uint32_t *>(sm + kOffUTmem);
-  int *const ek = reinterpret_cast<int *>(sm + kOffUScale);
-  uint32_t *const cm = reinterpret_cast<uint32_t *>(sm + kOffUScale + 256u);
-  const uint8_t *const bsrc = P.bop + ((size_t)pair * (ACCV ? 2u : 1u) + (isV ? 1u : 0u)) * kBopBytes;
+  double *const fk = reinterpret_cast<double *>(sm + kOffUScale);        // 2^(54 - e_k) of A's columns
+  double *const fo = fk + 64;                                             // 2^(h_j - 12) of C's columns
+  uint32_t *const cm = reinterpret_cast<uint32_t *>(sm + kOffUScale + 1024u); // [row quarter][column]
+  const int *const hcol = reinterpret_cast<const int *>(sm + kOffUB + kDig * kBPlane);
 
   if (tid == 0u) {
-    mbar_init(&bar[0], 1u);
-    mbar_init(&bar[1], 1u);
+    for (unsigned i = 0u; i < 4u; ++i)
+      mbar_init(&bar[i], 1u);
     mbar_fence_init();
-  }
-  if (tid < 64u) {
-    const unsigned gc = (tid < kBW) ? iBlk * kBW + tid : jBlk * kBW + tid - kBW;
-    ek[tid] = col_exp(cmax[P.parity * P.ncol + gc]);
-    cm[tid] = 0u;
   }
   if (warp == 0u)
     tmem_alloc(tmem_holder);
@@ -781,112 +876,159 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
   tc_fence_after();
   const uint32_t tmem = *tmem_holder;
   const uint32_t sbase = smem_u32(sm);
-  if (tid == 0u) {
-    mbar_arrive_expect_tx(&bar[0], kUStage + kBopBytes);
-    tma_load_2d(sm + kOffUStage, tm, (int)row0, (int)(iBlk * kBW), &bar[0]);
-    tma_load_2d(sm + kOffUStage + kUStage / 2u, tm, (int)row0, (int)(jBlk * kBW), &bar[0]);
-    bulk_g2s(sm + kOffUB, bsrc, kBopBytes, &bar[0]);
-  }
-  const bool ok_load = mbar_wait_bounded(&bar[0], 0u, kWait);
-  if (__syncthreads_or(!ok_load)) {
-    if (tid == 0u)
-      set_err(P);
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 0u)
-      tmem_dealloc(tmem);
-    return;
-  }
-  // slicing: thread takes rows r = tid % 128 of pair columns 16 kg .. 16 kg + 15, kg = tid / 128 and + 2
-  {
-    const double *const st = reinterpret_cast<const double *>(sm + kOffUStage);
-    const unsigned r = tid & 127u;
-#pragma unroll 1
-    for (unsigned kg = tid >> 7; kg < 4u; kg += 2u) {
-      long long w[16];
-#pragma unroll
-      for (unsigned i = 0u; i < 16u; ++i) {
-        const unsigned k = 16u * kg + i;
-        w[i] = biased_int(st[k * 128u + r], ek[k]);
-      }
-      uint4 pl[kDig];
-      digits16(w, pl);
-      uint8_t *const dst = sm + kOffUA + (r >> 3) * 512u + kg * 128u + (r & 7u) * 16u;
-#pragma unroll
-      for (unsigned t = 0u; t < kDig; ++t)
-        *reinterpret_cast<uint4 *>(dst + t * kUAPlane) = pl[t];
+  if (tid == 0u)
+    for (unsigned k = it0; k < it1 && k < it0 + 2u; ++k)
+      load_tile(P, item_of(P, k), sm + kOffUStage + (k - it0) * kUStage, &bar[k - it0]);
+
+  unsigned key = ~0u, nb = 0u; // the B operand held, and how many were loaded
+  bool failed = false;
+  // the next item's column maxima, loaded one item ahead (threads 0..63)
+  auto col_word = [&](const Item &x) -> uint32_t {
+    const unsigned gc = (tid < kBW) ? x.iBlk * kBW + tid : x.jBlk * kBW + tid - kBW;
+    return (x.isV ? P.cmaxV : P.cmaxG)[P.parity * P.ncol + gc];
+  };
+  uint32_t next_cmax = (tid < 64u && it0 < it1) ? col_word(item_of(P, it0)) : 0u;
+  for (unsigned k = it0, n = 0u; k < it1; ++k, ++n) {
+    const Item it = item_of(P, k);
+    const unsigned buf = n & 1u;
+    uint32_t *const cmax = it.isV ? P.cmaxV : P.cmaxG;
+    if (tid < 64u)
+      fk[tid] = cut_factor(col_exp(next_cmax));
+    const bool rec = blockIdx.x == 0u && tid == 0u;
+    long long c0 = rec ? clock64() : 0;
+    const bool newb = it.key != key;
+    if (newb && tid == 0u) { // the previous item's MMAs are complete: B is free
+      mbar_arrive_expect_tx(&bar[2], kBopBytes);
+      bulk_g2s(sm + kOffUB, P.bop + ((size_t)it.pair * (ACCV ? 2u : 1u) + (it.isV ? 1u : 0u)) * kBopBytes,
+               kBopBytes, &bar[2]);
     }
-  }
-  fence_async_shared();
-  __syncthreads();
-  if (tid == 0u) {
-    tc_fence_after();
-    constexpr uint32_t kId = idesc_i8(128u, 64u);
+    __syncthreads();
+    int bad = !mbar_wait_bounded(&bar[buf], (n >> 1) & 1u, kWait);
+    if (newb && !mbar_wait_bounded(&bar[2], nb & 1u, kWait))
+      bad = 1;
+    if (__syncthreads_or(bad)) {
+      failed = true;
+      break;
+    }
+    if (newb) {
+      key = it.key;
+      ++nb;
+      if (tid < 64u)
+        fo[tid] = p2(hcol[tid] - 12);
+    }
+    long long c1 = rec ? clock64() : 0;
+    // cut the tile into the digit planes of A: row r, pair columns 16 kg .. 16 kg + 15
+    {
+      const double *const st = reinterpret_cast<const double *>(sm + kOffUStage + buf * kUStage);
+      const unsigned r = tid & 127u;
 #pragma unroll 1
-    for (unsigned t = 0u; t < kDig; ++t)
-#pragma unroll 1
-      for (unsigned u = 0u; u + t < kDig; ++u)
-#pragma unroll 1
-        for (unsigned kh = 0u; kh < 2u; ++kh) {
-          const uint64_t a = sdesc(sbase + kOffUA + t * kUAPlane + kh * 256u, 128u, 512u);
-          const uint64_t b = sdesc(sbase + kOffUB + u * kBPlane + kh * 256u, 128u, 512u);
-          mma_i8(tmem + (t + u) * 64u, a, b, kId, (t == 0u && kh == 0u) ? 0u : 1u);
+      for (unsigned kg = tid >> 7; kg < 4u; kg += 2u) {
+        long long w[16];
+#pragma unroll
+        for (unsigned i = 0u; i < 16u; ++i) {
+          const unsigned c = 16u * kg + i;
+          w[i] = biased_int(st[c * 128u + r], fk[c]);
         }
-    mma_commit(&bar[1]);
-  }
-  const bool ok_mma = mbar_wait_bounded(&bar[1], 0u, kWait);
-  const bool failed = __syncthreads_or(!ok_mma) != 0;
-  tc_fence_after();
-  if (!failed) {
-    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. (rows of the tile), columns 32 (w / 4) ..
-    const unsigned q4 = warp & 3u, half = warp >> 2, r = q4 * 32u + lane;
-    const int *const h = reinterpret_cast<const int *>(sm + kOffUB + kDig * kBPlane);
-    double *const st = reinterpret_cast<double *>(sm + kOffUStage);
+        uint4 pl[kDig];
+        digits16(w, pl);
+        uint8_t *const dst = sm + kOffUA + (r >> 3) * 512u + kg * 128u + (r & 7u) * 16u;
+#pragma unroll
+        for (unsigned t = 0u; t < kDig; ++t)
+          *reinterpret_cast<uint4 *>(dst + t * kUAPlane) = pl[t];
+      }
+    }
+    fence_async_shared();
+    __syncthreads();
+    long long c2 = rec ? clock64() : 0;
+    if (tid < 64u && k + 1u < it1)
+      next_cmax = col_word(item_of(P, k + 1u));
+    if (tid == 0u) {
+      if (k + 2u < it1) // the tile is cut: its buffer takes the item two ahead
+        load_tile(P, item_of(P, k + 2u), sm + kOffUStage + buf * kUStage, &bar[buf]);
+      tc_fence_after();
+      // A = digit plane t of the tile (K half kh), B = planes u0 .. u0 + n - 1
+      // of V_loc side by side: D block t + u0 + i gets group t + u0 + i
+      const uint64_t a0 = sdesc(sbase + kOffUA, 128u, 512u), b0 = sdesc(sbase + kOffUB, 128u, 512u);
+#pragma unroll
+      for (unsigned kh = 0u; kh < 2u; ++kh) {
+#define GJX_UMMA(T, U0, NN)                                                                                          \
+  mma_i8(tmem + ((T) + (U0)) * 64u, a0 + (((T) * kUAPlane + kh * 256u) >> 4),                                        \
+         b0 + (((U0) * kBPlane + kh * 256u) >> 4), idesc_i8(128u, (NN) * 64u), ((T) == 0u && kh == 0u) ? 0u : 1u)
+        GJX_UMMA(0u, 0u, 4u);
+        GJX_UMMA(0u, 4u, 3u);
+        GJX_UMMA(1u, 0u, 4u);
+        GJX_UMMA(1u, 4u, 2u);
+        GJX_UMMA(2u, 0u, 4u);
+        GJX_UMMA(2u, 4u, 1u);
+        GJX_UMMA(3u, 0u, 4u);
+        GJX_UMMA(4u, 0u, 3u);
+        GJX_UMMA(5u, 0u, 2u);
+        GJX_UMMA(6u, 0u, 1u);
+#undef GJX_UMMA
+      }
+      mma_commit(&bar[3]);
+    }
+    if (__syncthreads_or(!mbar_wait_bounded(&bar[3], n & 1u, kWait))) {
+      failed = true;
+      break;
+    }
+    tc_fence_after();
+    long long c3 = rec ? clock64() : 0;
+    {
+      // warp w: TMEM lanes 32 (w % 4) .. (tile rows), output columns 32 (w / 4) ..
+      // in two chunks of 16 (each within one block of the pair)
+      const unsigned q4 = warp & 3u, half = warp >> 2, r = q4 * 32u + lane;
+      double *const out = it.isV ? P.V : P.G;
+      const size_t ld = it.isV ? P.ldV : P.ldG;
+      const bool inside = it.row0 + r < it.rows;
 #pragma unroll 1
-    for (unsigned ch = 0u; ch < 2u; ++ch) {
-      int acc[kDig][16];
-#pragma unroll
-      for (unsigned g = 0u; g < kDig; ++g)
-        tmem_ld16(tmem + ((q4 * 32u) << 16) + g * 64u + half * 32u + ch * 16u, acc[g]);
-      tmem_wait_ld();
-#pragma unroll
-      for (unsigned k = 0u; k < 16u; ++k) {
-        const unsigned j = half * 32u + ch * 16u + k;
-        int sg[kDig];
+      for (unsigned ch = 0u; ch < 2u; ++ch) {
+        const unsigned j0 = half * 32u + ch * 16u;
+        int acc[kDig][16];
 #pragma unroll
         for (unsigned g = 0u; g < kDig; ++g)
-          sg[g] = acc[g][k];
-        const double c = scale2(recombine(sg), h[j] - 12);
-        st[j * 128u + r] = c;
-        // rows beyond the matrix (zero-filled input) give 0 and change no maximum
-        const uint32_t m = __reduce_max_sync(0xffffffffu, abs_hi(c));
-        if (lane == 0u)
-          atomicMax(&cm[j], m);
+          tmem_ld16(tmem + ((q4 * 32u) << 16) + g * 64u + j0, acc[g]);
+        double f[16];
+#pragma unroll
+        for (unsigned kk = 0u; kk < 16u; ++kk)
+          f[kk] = fo[j0 + kk];
+        double *const col0 = out + ((half ? it.jBlk : it.iBlk) * kBW + ch * 16u) * ld + it.row0 + r;
+        tmem_wait_ld();
+#pragma unroll
+        for (unsigned kk = 0u; kk < 16u; ++kk) {
+          const double c = recombine_u(acc[0][kk], acc[1][kk], acc[2][kk], acc[3][kk], acc[4][kk], acc[5][kk],
+                                       acc[6][kk]) * f[kk];
+          if (inside)
+            col0[kk * ld] = c;
+          const uint32_t m = __reduce_max_sync(0xffffffffu, abs_hi(c)); // rows beyond the matrix hold 0
+          if (lane == 0u)
+            cm[q4 * 64u + j0 + kk] = m;
+        }
       }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (rec) {
+      const long long c4 = clock64();
+      P.clk[5] += c1 - c0;
+      P.clk[6] += c2 - c1;
+      P.clk[7] += c3 - c2;
+      P.clk[8] += c4 - c3;
+      P.clk[9] += 1;
+    }
+    if (tid < 64u) {
+      const uint32_t m = max(max(cm[tid], cm[64u + tid]), max(cm[128u + tid], cm[192u + tid]));
+      const unsigned gc = (tid < kBW) ? it.iBlk * kBW + tid : it.jBlk * kBW + tid - kBW;
+      if (m)
+        atomicMax(&cmax[(P.parity ^ 1u) * P.ncol + gc], m);
     }
   }
   tc_fence_before();
-  fence_async_shared();
   __syncthreads();
   if (warp == 0u)
     tmem_dealloc(tmem);
-  if (failed) {
-    if (tid == 0u)
-      set_err(P);
-    return;
-  }
-  if (tid == 0u) {
-    tma_store_2d(tm, sm + kOffUStage, (int)row0, (int)(iBlk * kBW));
-    tma_store_2d(tm, sm + kOffUStage + kUStage / 2u, (int)row0, (int)(jBlk * kBW));
-    bulk_commit();
-  }
-  if (tid < 64u) {
-    const unsigned gc = (tid < kBW) ? iBlk * kBW + tid : jBlk * kBW + tid - kBW;
-    if (cm[tid])
-      atomicMax(&cmax[(P.parity ^ 1u) * P.ncol + gc], cm[tid]);
-  }
-  if (tid == 0u)
-    bulk_wait_all();
+  if (failed && tid == 0u)
+    set_err(P);
 }
 
 // the largest |entry| of every column (high words), one warp per column
@@ -932,9 +1074,12 @@ struct SplitCtx {
   uint8_t *d_bop = nullptr;
   size_t bop_cap = 0u;
   unsigned long long *d_cnt = nullptr, *h_cnt = nullptr;
+  long long *d_clk = nullptr;  // 16 words: phase clocks of the last pair launch, update phase sums
+  std::vector<cudaEvent_t> ev; // profiling: two per outer step
 };
 std::mutex g_split_mtx;
 std::vector<SplitCtx> g_split_dev;
+long long *g_last_clk = nullptr; // the clock words of the last call's device
 thread_local std::string g_split_err;
 
 int cuda_fail(const cudaError_t e, const char *what)
@@ -998,21 +1143,30 @@ template <bool S, bool A> cudaError_t set_attrs()
   return cudaFuncSetAttribute(sp_update_kernel<A>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmem);
 }
 
-template <bool S, bool A> cudaError_t launch_step(const Params &p, const cudaStream_t st)
+template <bool S, bool A>
+cudaError_t launch_step(const Params &p, const cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1)
 {
   sp_pair_kernel<S, A><<<p.pairs, kThreads, kPairSmem, st>>>(p);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     return e;
-  sp_update_kernel<A><<<dim3(p.tilesG + p.tilesV, p.pairs), kThreads, kUpdSmem, st>>>(p);
-  return cudaGetLastError();
+  if (e0 && (e = cudaEventRecord(e0, st)) != cudaSuccess)
+    return e;
+  const unsigned items = p.pairs * (p.tilesG + p.tilesV);
+  sp_update_kernel<A><<<items < p.sms ? items : p.sms, kThreads, kUpdSmem, st>>>(p);
+  if ((e = cudaGetLastError()) != cudaSuccess)
+    return e;
+  return e1 ? cudaEventRecord(e1, st) : cudaSuccess;
 }
 
-cudaError_t launch_split_step(const bool sort, const bool accv, const Params &p, const cudaStream_t st)
+// one outer step: the pair kernel, then the update kernel (between events
+// e0 and e1 when profiling)
+cudaError_t launch_split_step(const bool sort, const bool accv, const Params &p, const cudaStream_t st,
+                              cudaEvent_t e0, cudaEvent_t e1)
 {
   if (sort)
-    return accv ? launch_step<true, true>(p, st) : launch_step<true, false>(p, st);
-  return accv ? launch_step<false, true>(p, st) : launch_step<false, false>(p, st);
+    return accv ? launch_step<true, true>(p, st, e0, e1) : launch_step<true, false>(p, st, e0, e1);
+  return accv ? launch_step<false, true>(p, st, e0, e1) : launch_step<false, false>(p, st, e0, e1);
 }
 
 int split_sweeps(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
@@ -1034,6 +1188,8 @@ int split_sweeps(const unsigned routine, const unsigned nrow, const unsigned nco
     SP_CUDA((set_attrs<false, false>()), "split kernel attributes");
     SP_CUDA(cudaMalloc(&c.d_s0, 64u * 64u), "cudaMalloc(split inner table)");
     SP_CUDA(cudaMalloc(&c.d_cnt, 2u * sizeof(unsigned long long)), "cudaMalloc(split counters)");
+    SP_CUDA(cudaMalloc(&c.d_clk, 16u * sizeof(long long)), "cudaMalloc(split clocks)");
+    SP_CUDA(cudaMemset(c.d_clk, 0, 16u * sizeof(long long)), "clear split clocks");
     SP_CUDA(cudaHostAlloc(&c.h_cnt, 2u * sizeof(unsigned long long), cudaHostAllocPortable), "cudaHostAlloc");
     c.configured = true;
   }
@@ -1083,6 +1239,12 @@ int split_sweeps(const unsigned routine, const unsigned nrow, const unsigned nco
   p.cmaxG = c.d_cmax;
   p.cmaxV = c.d_cmax + 2u * (size_t)ncol;
   p.bop = c.d_bop;
+  p.clk = c.d_clk;
+  g_last_clk = c.d_clk;
+  p.G = dG;
+  p.V = full ? dV : nullptr;
+  p.ldG = lddG;
+  p.ldV = full ? lddV : 0u;
   p.nrow = nrow;
   p.ncol = ncol;
   p.nplus = nplus;
@@ -1093,6 +1255,9 @@ int split_sweeps(const unsigned routine, const unsigned nrow, const unsigned nco
   p.tilesV = full ? (ncol + 127u) / 128u : 0u;
   p.gdefinite = (nplus ? ((nplus < ncol) ? 0 : +1) : -1);
   p.accv = full ? 1 : 0;
+  int nsm = 148;
+  SP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "SM count");
+  p.sms = (unsigned)nsm;
 
   if (full) {
     SP_CUDA(launch_initV(dV, ncol, lddV, st), "initV");
@@ -1102,20 +1267,39 @@ int split_sweeps(const unsigned routine, const unsigned nrow, const unsigned nco
   sp_colmax_kernel<<<(ncol + 7u) / 8u, 256u, 0u, st>>>(dG, nrow, ncol, lddG, p.cmaxG);
   SP_CUDA(cudaGetLastError(), "column maxima of G");
   SP_CUDA(cudaMemsetAsync(c.d_cnt + 1, 0, sizeof(unsigned long long), st), "clear error word");
+  SP_CUDA(cudaMemsetAsync(c.d_clk + 5, 0, 5u * sizeof(long long), st), "clear update clocks");
   *glb_s = 0ull;
   *glb_b = 0ull;
+  const bool prof = profiling();
+  if (prof)
+    while (c.ev.size() < 2u * c.steps1) {
+      cudaEvent_t e = nullptr;
+      SP_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+      c.ev.push_back(e);
+    }
+  profile_add(full ? 4u : 2u, 0u, 0.0); // initV, maxima of V; maxima of G, initD
   unsigned swp = 0u, gstep = 0u;
   while (swp < kNSweep) {
     SP_CUDA(cudaMemsetAsync(c.d_cnt, 0, sizeof(unsigned long long), st), "clear counter");
     for (unsigned s = 0u; s < c.steps1; ++s, ++gstep) {
       p.step = s;
       p.parity = gstep & 1u;
-      SP_CUDA(launch_split_step(cdsort, full, p, st), "split step");
+      SP_CUDA(launch_split_step(cdsort, full, p, st, prof ? c.ev[2u * s] : nullptr,
+                                prof ? c.ev[2u * s + 1u] : nullptr),
+              "split step");
     }
     ++swp;
     SP_CUDA(cudaMemcpyAsync(c.h_cnt, c.d_cnt, 2u * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
             "read counters");
     SP_CUDA(cudaStreamSynchronize(st), "split sweep");
+    double ms = 0.0;
+    if (prof)
+      for (unsigned s = 0u; s < c.steps1; ++s) {
+        float t = 0.0f;
+        SP_CUDA(cudaEventElapsedTime(&t, c.ev[2u * s], c.ev[2u * s + 1u]), "cudaEventElapsedTime");
+        ms += t;
+      }
+    profile_add(2ull * c.steps1, prof ? c.steps1 : 0u, ms);
     if ((int)c.h_cnt[1]) {
       set_error("a split-form kernel timed out waiting for its copies or products");
       return GJX_ERR_DEVICE;
@@ -1146,11 +1330,30 @@ extern "C" int gjx_hypJacL2_split(const unsigned routine, const unsigned nrow, c
     gjx::set_error("the split form takes ncol a multiple of 64 (blocks of 32 columns, an even number of them)");
     return -3;
   }
-  if (nrow > 61440u) {
-    gjx::set_error("the split form takes nrow <= 61440 (its int32 accumulators hold 8 x 4225 x nrow)");
+  if (nrow > gjx::split::kMaxRows) {
+    gjx::set_error("the split form takes nrow <= 16384 (its int32 Gram accumulators hold 7 x 2^14 x nrow)");
     return -2;
   }
   std::lock_guard<std::mutex> lk(gjx::g_split_mtx);
   return gjx::split_sweeps(routine, nrow, ncol, nplus, dG, lddG, dV, lddV, dD, static_cast<cudaStream_t>(stream),
                            glbSwp, glb_s, glb_b);
+}
+
+/* Cycles (clock64) from the start of block pair 0's CTA in the last
+ * sp_pair_kernel launch of the last gjx_hypJacL2_split call to the end of:
+ * [0] the Gram products, [1] the Gram epilogue, [2] the Cholesky factor,
+ * [3] the inner sweeps, [4] the B operands; then CTA 0 of the update kernel
+ * summed over the call: [5] waiting for its tile and B copies, [6] cutting
+ * the tiles, [7] the products, [8] the epilogues, [9] items.  0 or
+ * GJX_ERR_CUDA. */
+extern "C" int gjx_split_phase_cycles(long long *out10)
+{
+  std::lock_guard<std::mutex> lk(gjx::g_split_mtx);
+  if (!gjx::g_last_clk) {
+    for (int i = 0; i < 10; ++i)
+      out10[i] = 0;
+    return 0;
+  }
+  const cudaError_t e = cudaMemcpy(out10, gjx::g_last_clk, 10u * sizeof(long long), cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? 0 : GJX_ERR_CUDA;
 }

@@ -212,17 +212,26 @@ int gjx_hypJacL2_noalloc(const unsigned routine, const unsigned nrow, const unsi
  * tables for n1 = ncol / 32 outer and 64 inner columns), the Gram matrix of
  * each block pair and the update of G and V run as exact products of 8-bit
  * slices on the tensor cores (tcgen05 kind::i8, int32 accumulators),
- * recombined in FP64: 8 digits of 7 bits per entry, scaled per column by its
- * largest entry, the slice products of digit weight above 2^-56 kept.  The
+ * recombined in FP64: 7 digits of 8 bits per entry (55 bits), scaled per
+ * column by its largest entry, the slice products of weight above 2^-56 kept.  The
  * Cholesky factors, rotations, convergence test and D stay FP64.  The
  * results are not the plain form's bits; their accuracy is that of FP64
  * arithmetic (tests report it against LAPACK and the plain form).  ncol a
- * multiple of 64, nrow <= 61440; other codes as gjx_hypJacL2_dev.
+ * multiple of 64, nrow <= 16384; other codes as gjx_hypJacL2_dev.
  */
 int gjx_hypJacL2_split(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
                        double *const dG, const unsigned lddG, double *const dV, const unsigned lddV,
                        double *const dD, void *const stream, unsigned *const glbSwp,
                        unsigned long long *const glb_s, unsigned long long *const glb_b);
+
+/* Profiling of the split form: clock64 cycles from the start of block pair
+ * 0's CTA in the last pair-kernel launch of the last gjx_hypJacL2_split call
+ * to the end of [0] the Gram products, [1] the Gram epilogue, [2] the
+ * Cholesky factor, [3] the inner sweeps, [4] the update's B operands; and
+ * CTA 0 of the update kernel, summed over that call: [5] waiting for its
+ * copies, [6] cutting tiles into digits, [7] the tensor-core products, [8] the
+ * epilogues, [9] the tiles it took.  0 or GJX_ERR_CUDA. */
+int gjx_split_phase_cycles(long long *out10);
 
 /* Frees the device buffers that hypJacL2 keeps between calls on the current
  * device (they are reused by the next call of the same or smaller size). */
