@@ -31,12 +31,26 @@
  *   - V = I                                  share/device_code_common.hpp:221-230
  *   - sweep driver and argument checks      1/HypJacL2.cu:13-202
  *   - strategy table loading                 share/HypJacL.cu:11-121, share/my_utils.cu:30-61
+ *   - QR factor of the pair (-DUSE_QR):      share/device_code_common_QR.hpp:4-94 (dPeelOff,
+ *     Householder QR of 32-row chunks merged  dFactorize), share/device_code_common_Kepler.hpp:326-371
+ *     by Givens rotations                     (dQR32), share/device_code_common_rotate.hpp:120-155
+ *                                            (dGivens)
+ *   - scaled norms and cosines (-DUSE_QR,    share/device_code_common_Kepler.hpp:76-324 (dMax32,
+ *     -DUSE_DRMAC)                            dMin32, dSSQ32, dNRM2_32, dCOSA),
+ *                                            share/device_code_common_scale.hpp:7-58
+ *   - Drmac's inner sweep for the definite   share/device_code_cdsort_Drmac.hpp:4-316,
+ *     sorting kernels (-DUSE_DRMAC)           share/device_code_common_rotate.hpp:5-8 (tCot2)
+ *
+ * The variant (gjxo_set_variant): 0 the default build (Gram + Cholesky), 1
+ * the -DUSE_QR build, 2 the -DUSE_DRMAC build (which implies USE_QR).
  *
  * Build: gcc -O2 -fopenmp -ffp-contract=off -fno-fast-math (no contraction of
  * a*b+c into fma anywhere: every fma below is explicit).
  */
 
 #include <dlfcn.h>
+#include <float.h>
+#include <limits.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -48,6 +62,15 @@
 #endif
 
 #define O_NSWEEP 30u
+
+/* the two products of a Givens rotation in dPeelOff (c a + s b, c b - s a),
+ * as the reference's nvcc build contracts them */
+#ifndef O_GIVENS_A
+#define O_GIVENS_A(c, a, s, b) fma((c), (a), (s) * (b))
+#endif
+#ifndef O_GIVENS_B
+#define O_GIVENS_B(c, b, s, a) fma((c), (b), -((s) * (a)))
+#endif
 #define O_NCOLB 16u
 
 /* sqrt(2^-53), 2^27 = sqrt(2 / 2^-53), sqrt(32) * 2^-53, 2/sqrt(3), 1/2:
@@ -199,10 +222,416 @@ int gjxo_rotH(const double Apq, const double Dp, const double Dq, double *const 
 }
 
 /* ---------------------------------------------------------------------- */
-/* block-pair (L1) building blocks                                         */
+/* the variant builds: QR factor, scaled norms, Drmac's inner sweep          */
 /* ---------------------------------------------------------------------- */
 
 #define E32(A, r, c) (A)[(c) * 32u + (r)]
+
+static int o_variant = 0; /* 0 Cholesky, 1 QR, 2 Drmac (+ QR) */
+static void o_swap(double *const X, const unsigned p, const unsigned q);
+
+void gjxo_set_variant(const int v) { o_variant = v; }
+
+/* share/HypJacL.hpp:55-90: the decimal literals of the reference */
+static const double O_MU_ = 1.4916681462400414314624091158735E-154;
+static const double O_NU_ = 2.370187977027293260705088939015E+153;
+static const double O_MU_EPS = 1.0020841800044863889980540256751E-292;
+static const double O_NU_8 = 2.24711641857789464E+307;
+
+/* max |x| and min |x| (x != 0) over the 32 lanes: order-free (exact) */
+static double o_max32(const double *const x)
+{
+  double m = fabs(x[0]);
+  for (unsigned l = 1u; l < 32u; ++l)
+    m = fmax(m, fabs(x[l]));
+  return m;
+}
+
+static double o_min32(const double *const x)
+{
+  double m = (x[0] == 0.0) ? DBL_MAX : fabs(x[0]);
+  for (unsigned l = 1u; l < 32u; ++l)
+    m = fmin(m, (x[l] == 0.0) ? DBL_MAX : fabs(x[l]));
+  return m;
+}
+
+/* the butterfly sum of the lanes' squares (each square rounded first) */
+static double o_ssq_lanes(const double *const x)
+{
+  double v[32];
+  for (unsigned l = 0u; l < 32u; ++l)
+    v[l] = x[l] * x[l];
+  return gjxo_sum32(v);
+}
+
+/* share/device_code_common_scale.hpp:7-58 */
+static int o_find_scl(const double x, const double t)
+{
+  int x_n, t_n;
+  const double x_m = frexp(x, &x_n);
+  const double t_m = frexp(t, &t_n);
+  return ((x <= t) ? ((t_n - x_n) + (x_m < t_m)) : ((t_n - x_n) - (x_m > t_m)));
+}
+
+static int o_find_scl2(const double x)
+{
+  const int scl = ilogb(x);
+  return (scl + (scl & 1));
+}
+
+static void o_normalize2(int *const scl, double *const ssq)
+{
+  const int scl_ = o_find_scl2(*ssq);
+  *scl += scl_;
+  *ssq = scalbn(*ssq, -scl_);
+}
+
+static int o_cmp_scl(const int s1, const int s2, const double x1, const double x2)
+{
+  if (s1 < s2)
+    return -1;
+  if (s2 < s1)
+    return 1;
+  if (x1 < x2)
+    return -1;
+  if (x2 < x1)
+    return 1;
+  return 0;
+}
+
+static void o_sum_scl(const int s1, const int s2, const double x1, const double x2, int *const s, double *const x)
+{
+  if (o_cmp_scl(s1, s2, x1, x2) <= 0) {
+    *s = s2;
+    *x = scalbn(x1, s1 - s2) + x2;
+  }
+  else {
+    *s = s1;
+    *x = scalbn(x2, s2 - s1) + x1;
+  }
+}
+
+/* the lanes' |x| selected (and scaled) into the three magnitude ranges
+ * (share/device_code_common_Kepler.hpp:178-208) */
+static double o_ssq_range(const double *const x, const int range, const int scl)
+{
+  double v[32];
+  for (unsigned l = 0u; l < 32u; ++l) {
+    const double a = fabs(x[l]);
+    if (range == 0)
+      v[l] = (a < O_MU_) ? scalbn(a, scl) : 0.0;
+    else if (range == 1)
+      v[l] = ((a >= O_MU_) && (a <= O_NU_)) ? a : 0.0;
+    else
+      v[l] = (a > O_NU_) ? scalbn(a, scl) : 0.0;
+  }
+  return o_ssq_lanes(v);
+}
+
+/* share/device_code_common_Kepler.hpp:210-268: ssq * 2^scl = sum of squares */
+static int o_SSQ32(double *const ssq, const double *const x)
+{
+  const double M = o_max32(x);
+  if (M == 0.0) {
+    *ssq = 0.0;
+    return INT_MIN;
+  }
+  const double m = o_min32(x);
+  const int lo = (m < O_MU_), hi = (M > O_NU_);
+  int sc0, sc1, sc2, scl;
+  double sq0, sq1, sq2;
+  if (hi) {
+    sc2 = o_find_scl(M, O_NU_);
+    sq2 = o_ssq_range(x, 2, sc2);
+    sc2 *= -2;
+    if (m > O_NU_) {
+      scl = sc2;
+      *ssq = sq2;
+    }
+    else {
+      sc1 = 0;
+      sq1 = o_ssq_range(x, 1, 0);
+      if (sq1 > 0.0) {
+        o_normalize2(&sc1, &sq1);
+        o_normalize2(&sc2, &sq2);
+        o_sum_scl(sc1, sc2, sq1, sq2, &scl, ssq);
+      }
+      else {
+        scl = sc2;
+        *ssq = sq2;
+      }
+    }
+  }
+  else if (lo) {
+    sc0 = o_find_scl(m, O_MU_);
+    sq0 = o_ssq_range(x, 0, sc0);
+    sc0 *= -2;
+    if (M < O_MU_) {
+      scl = sc0;
+      *ssq = sq0;
+    }
+    else {
+      sc1 = 0;
+      sq1 = o_ssq_range(x, 1, 0);
+      if (sq1 > 0.0) {
+        o_normalize2(&sc1, &sq1);
+        o_normalize2(&sc0, &sq0);
+        o_sum_scl(sc0, sc1, sq0, sq1, &scl, ssq);
+      }
+      else {
+        scl = sc0;
+        *ssq = sq0;
+      }
+    }
+  }
+  else {
+    scl = 0;
+    *ssq = o_ssq_lanes(x);
+  }
+  return scl;
+}
+
+/* share/device_code_common_Kepler.hpp:278-283 */
+double gjxo_nrm2_32(const double *const x)
+{
+  double ssq;
+  const int scl = o_SSQ32(&ssq, x) / 2;
+  return scalbn(sqrt(ssq), scl);
+}
+
+/* share/device_code_common_Kepler.hpp:285-324 (Ap >= Aq in o_cosa_) */
+static double o_cosa_(const double Ap, const double Aq, const double *const x, const double *const y)
+{
+  double z[32];
+  int big, small;
+  if (Aq >= 1.0) {
+    big = ((Ap * Aq) >= DBL_MAX);
+    small = 0;
+  }
+  else {
+    big = 0;
+    small = ((Ap * Aq) <= O_MU_EPS);
+  }
+  if (big) {
+    for (unsigned l = 0u; l < 32u; ++l)
+      z[l] = (fabs(x[l]) >= fabs(y[l])) ? ((x[l] / Ap) * y[l]) : ((y[l] / Ap) * x[l]);
+    return gjxo_sum32(z) / Aq;
+  }
+  if (small) {
+    for (unsigned l = 0u; l < 32u; ++l)
+      z[l] = (fabs(x[l]) >= fabs(y[l])) ? (x[l] * (y[l] / Aq)) : (y[l] * (x[l] / Aq));
+    return gjxo_sum32(z) / Ap;
+  }
+  for (unsigned l = 0u; l < 32u; ++l)
+    z[l] = x[l] * y[l];
+  return (gjxo_sum32(z) / Aq) / Ap;
+}
+
+double gjxo_cosa(const double Ap, const double Aq, const double *const x, const double *const y)
+{
+  return (Ap >= Aq) ? o_cosa_(Ap, Aq, x, y) : o_cosa_(Aq, Ap, y, x);
+}
+
+/* share/device_code_common_rotate.hpp:120-155 */
+static void o_givens(const double f, const double g, double *const c, double *const s, double *const r)
+{
+  const double f_ = fabs(f), g_ = fabs(g);
+  if (f_ >= g_) {
+    if (g_ == 0.0) {
+      *c = copysign(1.0, f);
+      *s = 0.0;
+      *r = f_;
+    }
+    else {
+      const double g_f = g_ / f_;
+      *r = f_ * sqrt(fma(g_f, g_f, 1.0));
+      *c = f / *r;
+      *s = g / *r;
+    }
+  }
+  else {
+    if (f_ == 0.0) {
+      *c = 0.0;
+      *s = copysign(1.0, g);
+      *r = g_;
+    }
+    else {
+      const double f_g = f_ / g_;
+      *r = g_ * sqrt(fma(f_g, f_g, 1.0));
+      *c = f / *r;
+      *s = g / *r;
+    }
+  }
+}
+
+/* share/device_code_common_Kepler.hpp:326-371: Householder QR of a 32 x 32
+ * block, reflector k applied to columns k+1..31, column k set to -beta e_k */
+void gjxo_qr32(double *const A)
+{
+  for (unsigned k = 0u; k < 31u; ++k) {
+    double Axk[32], Axk_[32];
+    for (unsigned x = 0u; x < 32u; ++x) {
+      Axk[x] = E32(A, x, k);
+      Axk_[x] = (x >= k) ? Axk[x] : 0.0;
+    }
+    const double nrm2 = gjxo_nrm2_32(Axk_);
+    if (!(nrm2 > 0.0))
+      continue;
+    const double alpha = E32(A, k, k);
+    const double beta = copysign(nrm2, alpha);
+    const double alpha_beta = alpha + beta;
+    const double tau = alpha_beta / beta;
+    double Vxk[32];
+    for (unsigned x = 0u; x < 32u; ++x)
+      Vxk[x] = (x == k) ? 1.0 : ((x > k) ? (Axk_[x] / alpha_beta) : 0.0);
+    for (unsigned j = k + 1u; j < 32u; ++j) {
+      double v[32];
+      for (unsigned x = 0u; x < 32u; ++x)
+        v[x] = Vxk[x] * E32(A, x, j);
+      const double dp = gjxo_sum32(v);
+      const double _tdp = -(tau * dp);
+      for (unsigned x = 0u; x < 32u; ++x)
+        E32(A, x, j) = fma(_tdp, Vxk[x], E32(A, x, j));
+    }
+    for (unsigned x = 0u; x < 32u; ++x)
+      E32(A, x, k) = (x == k) ? -beta : ((x > k) ? 0.0 : Axk[x]);
+  }
+}
+
+/* share/device_code_common_QR.hpp:4-66: the triangular R1 (a QR-factored
+ * chunk) merged into R0 by Givens rotations along the diagonals: in step k
+ * row x of R0 and row x - k of R1 (x >= k) are rotated so that R1(x-k, x)
+ * vanishes, in every column >= x */
+static void o_peel(double *const R0, double *const R1)
+{
+  for (unsigned k = 0u; k < 32u; ++k)
+    for (unsigned x = k; x < 32u; ++x) {
+      const unsigned xk = x - k;
+      double c, s, r;
+      o_givens(E32(R0, x, x), E32(R1, xk, x), &c, &s, &r);
+      for (unsigned j = x + 1u; j < 32u; ++j) {
+        const double a = E32(R0, x, j), b = E32(R1, xk, j);
+        E32(R0, x, j) = O_GIVENS_A(c, a, s, b);
+        E32(R1, xk, j) = O_GIVENS_B(c, b, s, a);
+      }
+      E32(R0, x, x) = r;
+      E32(R1, xk, x) = 0.0;
+    }
+}
+
+/* share/device_code_common_QR.hpp:68-92 (dFactorize): R of the pair's rows */
+void gjxo_qr_factor(double *const Gi, double *const Gj, const size_t ld, const unsigned nrow, double *const A)
+{
+  double W[1024];
+  for (unsigned y = 0u; y < 32u; ++y)
+    for (unsigned x = 0u; x < 32u; ++x)
+      E32(A, x, y) = ((y < O_NCOLB) ? Gi + y * ld : Gj + (y - O_NCOLB) * ld)[x];
+  gjxo_qr32(A);
+  for (unsigned i = 32u; i < nrow; i += 32u) {
+    for (unsigned y = 0u; y < 32u; ++y)
+      for (unsigned x = 0u; x < 32u; ++x)
+        E32(W, x, y) = ((y < O_NCOLB) ? Gi + y * ld : Gj + (y - O_NCOLB) * ld)[i + x];
+    gjxo_qr32(W);
+    o_peel(A, W);
+  }
+}
+
+/* share/device_code_cdsort_Drmac.hpp:4-316: the definite sorting sweep with
+ * scaled norms and cosines; def = +1 (descending) or -1 (ascending) */
+static void o_drmac(double *const G, double *const V, const unsigned char *const strat0, const unsigned s0steps,
+                    const unsigned nswp, const int def, unsigned *const s, unsigned *const b)
+{
+  unsigned blk_s = 0u, blk_b = 0u;
+  for (unsigned swp = 0u; swp < nswp; ++swp) {
+    unsigned swp_s = 0u, swp_b = 0u;
+    for (unsigned step = 0u; step < s0steps; ++step)
+      for (unsigned y = 0u; y < 16u; ++y) {
+        const unsigned p = strat0[(step * 16u + y) * 2u + 0u];
+        const unsigned q = strat0[(step * 16u + y) * 2u + 1u];
+        double Gp[32], Gq[32], Vp[32], Vq[32];
+        for (unsigned x = 0u; x < 32u; ++x) {
+          Gp[x] = E32(G, x, p);
+          Gq[x] = E32(G, x, q);
+          Vp[x] = E32(V, x, p);
+          Vq[x] = E32(V, x, q);
+        }
+        const double Ap = gjxo_nrm2_32(Gp), Aq = gjxo_nrm2_32(Gq), CosA = gjxo_cosa(Ap, Aq, Gp, Gq);
+        const int transf_s = (fabs(CosA) >= O_MYTOL);
+        swp_s += (unsigned)transf_s;
+        int transf_b = 0;
+        if (transf_s) {
+          const double Aq_p = Aq / Ap, Ap_q = Ap / Aq, ct2 = (Aq_p - Ap_q) / scalbn(CosA, 1);
+          if (ct2 <= O_NU_8) {
+            const double CT2 = fabs(ct2);
+            double c, t;
+            if (CT2 < O_SQRT_HEPS) {
+              const double cot = CT2 + 1.0;
+              t = copysign(1.0 / cot, ct2);
+              c = gjxo_rsqrt_rn(fma(t, t, 1.0));
+              transf_b = 1;
+            }
+            else if (CT2 >= O_SQRT_2_HEPS) {
+              const double cot = scalbn(CT2, 1);
+              c = 1.0;
+              t = copysign(1.0 / cot, ct2);
+            }
+            else {
+              const double cot = CT2 + sqrt(fma(CT2, CT2, 1.0));
+              t = copysign(1.0 / cot, ct2);
+              c = gjxo_rsqrt_rn(fma(t, t, 1.0));
+              transf_b = (c < 1.0);
+            }
+            const double t_ = -t, tCosA = t * CosA, tCosA_ = -tCosA;
+            const double Ap_ = Ap * sqrt(fma(tCosA_, Aq_p, 1.0)), Aq_ = Aq * sqrt(fma(tCosA, Ap_q, 1.0));
+            const int keep = (def > 0) ? (Ap_ >= Aq_) : (Ap_ <= Aq_);
+            const unsigned dp = keep ? p : q, dq = keep ? q : p;
+            for (unsigned x = 0u; x < 32u; ++x) {
+              const double np = fma(t_, Gq[x], Gp[x]), nq = fma(t, Gp[x], Gq[x]);
+              const double mp = fma(t_, Vq[x], Vp[x]), mq = fma(t, Vp[x], Vq[x]);
+              E32(G, x, dp) = transf_b ? (c * np) : np;
+              E32(G, x, dq) = transf_b ? (c * nq) : nq;
+              E32(V, x, dp) = transf_b ? (c * mp) : mp;
+              E32(V, x, dq) = transf_b ? (c * mq) : mq;
+            }
+          }
+          else if ((def > 0) ? (Ap >= Aq) : (Ap <= Aq)) {
+            const double t_ = CosA, t = -t_;
+            for (unsigned x = 0u; x < 32u; ++x) {
+              E32(G, x, q) = Aq * fma(t, Gp[x] / Ap, Gq[x] / Aq);
+              E32(V, x, p) = fma(t_, Vq[x], Vp[x]);
+              E32(V, x, q) = fma(t, Vp[x], Vq[x]);
+            }
+          }
+          else {
+            const double t = CosA, t_ = -t;
+            for (unsigned x = 0u; x < 32u; ++x) {
+              E32(G, x, q) = Ap * fma(t_, Gq[x] / Aq, Gp[x] / Ap);
+              E32(G, x, p) = Gq[x];
+              E32(V, x, q) = fma(t_, Vq[x], Vp[x]);
+              E32(V, x, p) = fma(t, Vp[x], Vq[x]);
+            }
+          }
+        }
+        else if ((def > 0) ? (Ap < Aq) : (Aq < Ap)) {
+          o_swap(G, p, q);
+          o_swap(V, p, q);
+        }
+        swp_b += (unsigned)transf_b;
+      }
+    if (swp_s) {
+      blk_s += swp_s;
+      blk_b += swp_b;
+    }
+    else
+      break;
+  }
+  *s = blk_s;
+  *b = blk_b;
+}
+
+/* ---------------------------------------------------------------------- */
+/* block-pair (L1) building blocks                                         */
+/* ---------------------------------------------------------------------- */
 
 /* local column c of the pair [G_i G_j] */
 static inline double *o_col(double *const Gi, double *const Gj, const size_t ld, const unsigned c)
@@ -416,8 +845,12 @@ static void o_pair(const unsigned routine, const unsigned nrow, const unsigned n
   const int cdsort = (routine & 1u) != 0u, full = (routine & 2u) != 0u;
   double *const Gi = G + (size_t)iBlk * O_NCOLB * ldG, *const Gj = G + (size_t)jBlk * O_NCOLB * ldG;
   double A[1024], Vl[1024];
-  gjxo_gram(Gi, Gj, ldG, nrow, A);
-  gjxo_chol32(A);
+  if (o_variant) /* -DUSE_QR / -DUSE_DRMAC builds */
+    gjxo_qr_factor(Gi, Gj, ldG, nrow, A);
+  else {
+    gjxo_gram(Gi, Gj, ldG, nrow, A);
+    gjxo_chol32(A);
+  }
   for (unsigned i = 0u; i < 1024u; ++i)
     Vl[i] = ((i >> 5u) == (i & 31u)) ? 1.0 : 0.0;
 
@@ -452,7 +885,10 @@ static void o_pair(const unsigned routine, const unsigned nrow, const unsigned n
   }
 
   const int mode = cdsort ? (definite ? 2 : 3) : (definite ? 0 : 1);
-  gjxo_inner(A, Vl, strat0, s0steps, nswp0, mode, definite, npos, s, b);
+  if (mode == 2 && o_variant == 2)
+    o_drmac(A, Vl, strat0, s0steps, nswp0, definite, s, b);
+  else
+    gjxo_inner(A, Vl, strat0, s0steps, nswp0, mode, definite, npos, s, b);
 
   if (cdsort || *s) {
     gjxo_update(Gi, Gj, ldG, nrow, Vl);

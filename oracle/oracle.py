@@ -62,12 +62,34 @@ def lib():
         L.gjxo_outer_step.restype = None
         L.gjxo_load_strat.argtypes = [ctypes.c_char_p, ctypes.c_char_p, u, pu16, u]
         L.gjxo_load_strat.restype = i
+        L.gjxo_set_variant.argtypes = [i]
+        L.gjxo_set_variant.restype = None
+        L.gjxo_nrm2_32.argtypes = [pd]
+        L.gjxo_nrm2_32.restype = d
+        L.gjxo_cosa.argtypes = [d, d, pd, pd]
+        L.gjxo_cosa.restype = d
         _lib = L
     return _lib
 
 
 def _p(a, t=ctypes.c_double):
     return a.ctypes.data_as(ctypes.POINTER(t)) if a is not None else None
+
+
+VARIANTS = {"base": 0, "qr": 1, "drmac": 2}
+
+
+def set_variant(name: str) -> None:
+    """Which build of the reference to restate: "base" (Gram + Cholesky),
+    "qr" (-DUSE_QR: Householder/Givens factor), "drmac" (-DUSE_DRMAC: the QR
+    factor and Drmac's scaled-norm sweep in the definite sorting kernels)."""
+    lib().gjxo_set_variant(VARIANTS[name])
+
+
+def nrm2_32(v) -> float:
+    a = np.ascontiguousarray(v, dtype=np.float64)
+    assert a.size == 32
+    return lib().gjxo_nrm2_32(_p(a))
 
 
 def rsqrt_rn(x: float) -> float:

@@ -2,8 +2,10 @@
 
 tests/golden/ref_golden_base.json holds the outputs of the reference's own
 hypJacL2 (its sources built for sm_100a, run on a B200 by
-tests/golden/make_golden.py) on seeded inputs.  The oracle must reproduce
-every one bit for bit: U, V, D, the sweep count and both rotation counts.
+tests/golden/make_golden.py) on seeded inputs; ref_golden_qr.json and
+ref_golden_drmac.json those of its -DUSE_QR and -DUSE_DRMAC builds on the
+same inputs.  The oracle (in the matching variant) must reproduce every one
+bit for bit: U, V, D, the sweep count and both rotation counts.
 """
 
 import numpy as np
@@ -15,6 +17,7 @@ from tests.golden.make_golden import make_input
 
 GOLD = load_golden("base")
 CASES = GOLD["cases"] if GOLD else []
+VARIANT_CASES = [(v, c) for v in ("qr", "drmac") for c in (load_golden(v) or {"cases": []})["cases"]]
 
 
 def test_golden_present():
@@ -24,6 +27,24 @@ def test_golden_present():
 
 @pytest.mark.parametrize("c", CASES, ids=[c["name"] for c in CASES])
 def test_oracle_equals_reference(c, oracle, strat_path):
+    oracle.set_variant("base")
+    _check(c, oracle, strat_path)
+
+
+def test_variant_goldens_present():
+    assert len(VARIANT_CASES) == 2 * len(CASES)
+
+
+@pytest.mark.parametrize("v,c", VARIANT_CASES, ids=[f"{v}-{c['name']}" for v, c in VARIANT_CASES])
+def test_oracle_equals_reference_variant_builds(v, c, oracle, strat_path):
+    oracle.set_variant(v)
+    try:
+        _check(c, oracle, strat_path)
+    finally:
+        oracle.set_variant("base")
+
+
+def _check(c, oracle, strat_path):
     G = make_input(c)
     assert synth.digest(G) == c["input_sha"], "input generator drifted"
     s0 = oracle.load_strat(strat_path, c["snp0"], 32)
