@@ -112,6 +112,8 @@ def lib() -> ctypes.CDLL:
     L.gjx_set_split.restype = None
     L.gjx_set_pairs_per_cta.argtypes = [u]
     L.gjx_set_pairs_per_cta.restype = None
+    L.gjx_set_variant.argtypes = [u]
+    L.gjx_set_variant.restype = None
     L.gjx_set_sweep_mode.argtypes = [i]
     L.gjx_set_sweep_mode.restype = None
     L.gjx_configure_device.argtypes = [i]
@@ -255,6 +257,15 @@ def hypJacL2_dev(routine: int, G, nplus: int, V=None, D=None, stream=None, nrow:
     if check and ret:
         raise GjxError(ret, last_error() if ret > 0 else "invalid argument")
     return ret, swp.value, s.value, b.value
+
+
+VARIANTS = {"base": 0, "qr": 1, "drmac": 2}
+
+
+def set_variant(name: str) -> None:
+    """The pivot-block factor of the reference's builds to reproduce: "base"
+    (Gram + Cholesky), "qr" (-DUSE_QR), "drmac" (-DUSE_DRMAC)."""
+    lib().gjx_set_variant(VARIANTS[name])
 
 
 def hypJacL2_split(routine: int, G, nplus: int, V=None, D=None, stream=None, nrow: Optional[int] = None,

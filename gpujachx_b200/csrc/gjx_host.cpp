@@ -51,6 +51,7 @@ int g_verbose = 1;
 int g_sweep_mode = -1; // -1 automatic (the tuned choice, else per step), 0 per outer step, 1 one launch per sweep
 unsigned g_split = 0u;  // CTAs per block pair: 0 automatic (the tuned choice, else by the SM count), else 1, 2, 4
 unsigned g_pairs_per_cta = 0u; // block pairs a CTA takes at a time: 0 automatic, 1, or 2
+unsigned g_variant = 0u; // pivot-block factor: 0 Gram + Cholesky, 1 QR (-DUSE_QR), 2 QR + Drmac (-DUSE_DRMAC)
 
 // the autotuner's choices, by (routine, nrow, ncol, nplus)
 struct TuneKey {
@@ -240,6 +241,12 @@ int run_sweeps_core(const unsigned routine, const unsigned nrow, const unsigned 
   GJX_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
   GJX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
   p.width = (p.split == 1u && (g_pairs_per_cta == 2u || (!g_pairs_per_cta && p.pairs > (unsigned)sms))) ? 2u : 1u;
+  p.variant = g_variant;
+  if (p.variant) { // the QR factors: one CTA per block pair, one launch per outer step
+    p.split = 1u;
+    p.width = 1u;
+    mode = 0;
+  }
   GJX_CUDA(gjx::make_update_map(&p.tmG, dG, nrow, ncol, lddG), "tensor map of G");
   GJX_CUDA(gjx::make_gram_map(&p.tmGram, dG, nrow, ncol, lddG), "Gram tensor map of G");
   if (full)
@@ -1123,6 +1130,13 @@ int gjx_hypJacL2_batched(const unsigned routine, const unsigned nmat, const unsi
                          double *const *const dD, void *const stream, unsigned *const sweeps,
                          unsigned long long *const glb_s, unsigned long long *const glb_b, int *const info)
 {
+  {
+    std::lock_guard<std::mutex> lk(g_mtx);
+    if (g_variant) {
+      g_err = "the batched form takes the default pivot-block factor (gjx_set_variant(0))";
+      return -1;
+    }
+  }
   if (!nmat || nmat > 65535u || !nrow || !ncol || !nplus || !dG || !lddG || !dD || !sweeps || !glb_s || !glb_b ||
       !info || ((routine & GJX_FULL_SVD) && (!dV || !lddV)) || routine >= 16u) {
     g_err = "gjx_hypJacL2_batched: bad arguments";
@@ -1147,6 +1161,12 @@ void gjx_set_split(const unsigned n)
 {
   std::lock_guard<std::mutex> lk(g_mtx);
   g_split = (n == 1u || n == 2u || n == 4u) ? n : 0u;
+}
+
+void gjx_set_variant(const unsigned v)
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  g_variant = (v <= 2u) ? v : 0u;
 }
 
 void gjx_set_pairs_per_cta(const unsigned w)

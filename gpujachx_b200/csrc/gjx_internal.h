@@ -34,6 +34,7 @@ struct alignas(64) StepParams {
   unsigned width;               // with split 1: block pairs per CTA, 1 or 2 (l1_step2_kernel)
   unsigned steps1;              // outer steps per sweep (persistent sweep kernel)
   unsigned *ver;                // per block: CTAs that have finished writing it this sweep
+  unsigned variant;             // pivot-block factor: 0 Gram + Cholesky, 1 QR, 2 QR + Drmac's sweep
 };
 
 // one matrix of a batch: its step parameters (step unused) and D

@@ -46,6 +46,7 @@
 
 #include "gjx_device.cuh"
 #include "gjx_internal.h"
+#include "gjx_qr.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -763,10 +764,11 @@ __device__ __forceinline__ void add_counts(const StepParams &P, const unsigned b
 // ---------------------------------------------------------------------------
 // NBUF update buffers: 2 in the region of the Gram stages, a third (NBUF = 3)
 // at kOffUpd3 where the launch provides it
-template <bool SORT, bool ACCV, unsigned NSPLIT, unsigned NBUF = 2u>
+template <bool SORT, bool ACCV, unsigned NSPLIT, unsigned NBUF = 2u, unsigned FAC = 0u>
 __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned step, const unsigned pair,
                                           const unsigned rank, double *const sm)
 {
+  static_assert(FAC == 0u || NSPLIT == 1u, "the QR factor is one CTA's");
   static_assert(NBUF == 2u || NBUF == 3u, "2 or 3 update buffers");
   double *const stg = sm;
   double *const R = sm + kOffR;
@@ -788,6 +790,12 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
   }
   __syncthreads();
 
+  int failed = 0;
+  if constexpr (FAC != 0u) {
+    // ----------------- 1'. QR factor (the -DUSE_QR builds) -----------------
+    qr_factor_cta(P.G + (size_t)iBlk * kNColB * P.ldG, P.G + (size_t)jBlk * kNColB * P.ldG, P.ldG, P.nrow, R, stg);
+  }
+  else {
   // ------------------------------ 1. Gram --------------------------------
   const unsigned ntile = P.nrow >> 6; // 64-row tiles
   // chains per lane: 8 with one CTA per pair (gram_tile2), 4 with 2 CTAs
@@ -823,7 +831,6 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
     for (unsigned k = 0u; k + 1u < kGramStages && k < ngst; ++k)
       issue_gram(k);
   unsigned k = 0u;
-  int failed = 0;
   for (; k < ngst; ++k) {
     if (tid == kIssuer && k + kGramStages - 1u < ngst)
       issue_gram(k + kGramStages - 1u); // into the buffer released at the end of stage k - 1
@@ -879,6 +886,7 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
         }
       }
   }
+  }
   if (NSPLIT > 1u)
     cg::this_cluster().sync(); // release our writes, acquire the others'
   else
@@ -909,7 +917,8 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
   // ---------------------------- 2. Cholesky -------------------------------
   for (unsigned i = tid; i < 1024u; i += kThreads)
     Vl[i] = ((i >> 5) == (i & 31u)) ? 1.0 : 0.0;
-  chol32_grp<8u>(R, tid, 0u);
+  if constexpr (FAC == 0u)
+    chol32_grp<8u>(R, tid, 0u);
   __syncthreads();
 
   // --------------------------- 3. inner sweeps ----------------------------
@@ -917,7 +926,10 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
   unsigned npos;
   block_signature(P, iBlk, jBlk, definite, npos);
   unsigned blk_s, blk_b;
-  inner_sweeps<SORT, 8u>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, lane, warp, 0u, blk_s, blk_b);
+  if (FAC == 2u && SORT && definite) // -DUSE_DRMAC: Drmac's sweep in the definite sorting kernels
+    drmac_sweeps(R, Vl, s0, P.s0steps, P.nswp0, definite, red, lane, warp, blk_s, blk_b);
+  else
+    inner_sweeps<SORT, 8u>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, lane, warp, 0u, blk_s, blk_b);
 
   if (rank == 0u && tid == 0u)
     add_counts(P, blk_s, blk_b);
@@ -1276,6 +1288,15 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
   return v;
 }
 
+// the reference's alternative builds (P.variant: 1 -DUSE_QR, 2 -DUSE_DRMAC):
+// one CTA per block pair, the QR factor in place of the Gram and Cholesky
+template <bool SORT, bool ACCV, unsigned FAC>
+__global__ void __launch_bounds__(kThreads, 1) l1_var_kernel(const __grid_constant__ StepParams P)
+{
+  extern __shared__ __align__(128) double sm[];
+  pair_step<SORT, ACCV, 1u, 2u, FAC>(P, P.step, blockIdx.x, 0u, sm);
+}
+
 template <bool SORT, bool ACCV, unsigned NSPLIT>
 __global__ void __launch_bounds__(kThreads, 1) l1_sweep_kernel(const __grid_constant__ StepParams P)
 {
@@ -1599,10 +1620,20 @@ template <bool S, bool A> static cudaError_t set_smem2()
                               (int)batch2_smem_bytes());
 }
 
+template <bool S, bool A, unsigned F> static cudaError_t set_smem_var(const int bytes)
+{
+  return cudaFuncSetAttribute(l1_var_kernel<S, A, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
 cudaError_t l1_configure()
 {
   const int b = (int)l1_smem_bytes();
   cudaError_t e;
+  if ((e = set_smem_var<false, false, 1u>(b)) || (e = set_smem_var<false, true, 1u>(b)) ||
+      (e = set_smem_var<true, false, 1u>(b)) || (e = set_smem_var<true, true, 1u>(b)) ||
+      (e = set_smem_var<false, false, 2u>(b)) || (e = set_smem_var<false, true, 2u>(b)) ||
+      (e = set_smem_var<true, false, 2u>(b)) || (e = set_smem_var<true, true, 2u>(b)))
+    return e;
   if ((e = set_smem2<false, false>()) || (e = set_smem2<false, true>()) || (e = set_smem2<true, false>()) ||
       (e = set_smem2<true, true>()))
     return e;
@@ -1785,8 +1816,24 @@ template <bool S, bool A> static cudaError_t launch2(const StepParams &p, cudaSt
   return cudaGetLastError();
 }
 
+template <bool S, bool A, unsigned F> static cudaError_t launch_var(const StepParams &p, cudaStream_t s)
+{
+  l1_var_kernel<S, A, F><<<p.pairs, kThreads, l1_smem_bytes(), s>>>(p);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_l1_step(const bool sort, const bool accv, const StepParams &p, cudaStream_t s)
 {
+  if (p.variant == 1u) {
+    if (sort)
+      return accv ? launch_var<true, true, 1u>(p, s) : launch_var<true, false, 1u>(p, s);
+    return accv ? launch_var<false, true, 1u>(p, s) : launch_var<false, false, 1u>(p, s);
+  }
+  if (p.variant == 2u) {
+    if (sort)
+      return accv ? launch_var<true, true, 2u>(p, s) : launch_var<true, false, 2u>(p, s);
+    return accv ? launch_var<false, true, 2u>(p, s) : launch_var<false, false, 2u>(p, s);
+  }
   const unsigned n = p.split;
   if (n == 1u && p.width == 2u) {
     if (sort)

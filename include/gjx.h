@@ -116,6 +116,17 @@ void gjx_set_split(unsigned n);
  * same bits for every value. */
 void gjx_set_pairs_per_cta(unsigned w);
 
+/* The pivot-block factor of the reference's alternative builds, for
+ * hypJacL2, gjx_hypJacL2_dev and gjx_hypJacL2_noalloc: 0 (default) the Gram
+ * matrix and its Cholesky factor (share/device_code_common_Cholesky.hpp);
+ * 1 as the -DUSE_QR build: Householder QR of the pair's 32-row chunks merged
+ * by Givens rotations (share/device_code_common_QR.hpp:4-94,
+ * share/device_code_common_Kepler.hpp:326-371); 2 as the -DUSE_DRMAC build:
+ * the QR factor and Drmac's scaled-norm sweep in the definite sorting case
+ * (share/device_code_cdsort_Drmac.hpp:4-316).  Each gives the bits of that
+ * build.  Values above 2 select 0.  The batched form refuses 1 and 2. */
+void gjx_set_variant(unsigned v);
+
 /*
  * Autotuner: time every launch configuration of this shape -- 1, 2 or 4
  * CTAs per block pair (where the pairs fit), one launch per outer step or
