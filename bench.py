@@ -472,8 +472,10 @@ def main_batch(args):
         G0, offs = batch_inputs(sizes, dev, cfg["seed"] + rank)
     nplus = [int(n) if b % 2 == 0 else int(n) // 2 for b, n in enumerate(sizes)]
     g.init_strats(None, "cycwor", 32, "cycwor", 4)
-    width = 1 if os.environ.get("GJX_PAIRS_PER_CTA") == "1" else 2  # block pairs per CTA at a time
-    g.lib().gjx_set_pairs_per_cta(width)
+    # the library's batched autotuner, once per batch shape, before timing:
+    # block pairs per CTA and one launch per step index or per sweep
+    tuned = g.autotune_batched(ALG, [int(n) for n in sizes], [int(n) for n in sizes], nplus)
+    width = tuned["pairs_per_cta"]
     dG = torch.empty_like(G0)
     dV = torch.empty_like(G0)
     dD = torch.empty(int(sizes.sum()), dtype=torch.float64, device=dev)
@@ -521,7 +523,9 @@ def main_batch(args):
     t_s = statistics.median(times) / 1000.0
     hbm, peak_kind = _peaks()
     roof = {"bound": "hbm", "achieved": nbytes / t_s / 1e9, "peak": hbm, "unit": "GB/s",
-            "frac": nbytes / t_s / 1e9 / hbm, "traffic": None, "kernel": f"gjx::l1_batch_kernel<true,true,{width}>",
+            "frac": nbytes / t_s / 1e9 / hbm, "traffic": None,
+            "kernel": ("gjx::l1_batch_flow_kernel<true,true,%d>" if tuned["mode"] else "gjx::l1_batch_kernel<true,true,%d>")
+            % width,
             "peak_kind": f"{peak_kind} HBM copy bandwidth",
             "note": "algorithmic bytes of all sweeps run, over the device time of the whole batched call",
             "fp64_tflops": flops / t_s / 1e12, "launches_per_step": prof["launches"] // max(1, args.steps)}
@@ -554,6 +558,7 @@ def main_batch(args):
             "data": "synthetic",
             "config": {"workload": cfg["workload"], "name": "c5", "count": nmat, "alg": ALG,
                        "block_pairs_per_cta": width,
+                       "launches": "one per sweep" if tuned["mode"] else "one per outer step index",
                        "parallelism": ("one batch partitioned over ranks (size-balanced)" if (args.shard and world > 1)
                                        else "independent batches per rank" if world > 1 else "single GPU"),
                        "l2": "flushed between steps (256 MiB write, outside the timed events); inputs 3.4 GB > L2"},

@@ -114,6 +114,10 @@ def lib() -> ctypes.CDLL:
     L.gjx_set_pairs_per_cta.restype = None
     L.gjx_set_variant.argtypes = [u]
     L.gjx_set_variant.restype = None
+    L.gjx_set_batch_mode.argtypes = [i]
+    L.gjx_set_batch_mode.restype = None
+    L.gjx_autotune_batched.argtypes = [u, u, pu, pu, pu, u, pu]
+    L.gjx_autotune_batched.restype = i
     L.gjx_set_sweep_mode.argtypes = [i]
     L.gjx_set_sweep_mode.restype = None
     L.gjx_configure_device.argtypes = [i]
@@ -322,6 +326,21 @@ def hypJacL2_batched(routine: int, Gs, nplus, Vs=None, Ds=None, stream=None, nro
     if ret:
         raise GjxError(ret, last_error())
     return BatchResult(ret, list(info), list(sw), list(rs), list(rb))
+
+
+def autotune_batched(routine: int, nrows, ncols, nplus, sweeps: int = 1) -> dict:
+    """Time the batched form's configurations (block pairs per CTA, launch per
+    step or per sweep) on seeded random matrices of these shapes and keep the
+    fastest for later batches of the same shapes (gjx_autotune_batched);
+    returns {"pairs_per_cta": 1 or 2, "mode": 0 per step / 1 per sweep}."""
+    n = len(ncols)
+    U = ctypes.c_uint * n
+    out = (ctypes.c_uint * 2)()
+    npl = list(nplus) if hasattr(nplus, "__len__") else [int(nplus)] * n
+    r = lib().gjx_autotune_batched(routine, n, U(*nrows), U(*ncols), U(*npl), sweeps, out)
+    if r:
+        raise GjxError(r, last_error() if r > 0 else "invalid argument")
+    return {"pairs_per_cta": out[0], "mode": out[1]}
 
 
 def autotune(routine: int, nrow: int, ncol: int, nplus: int, sweeps: int = 1) -> dict:

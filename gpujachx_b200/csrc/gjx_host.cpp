@@ -52,6 +52,10 @@ int g_sweep_mode = -1; // -1 automatic (the tuned choice, else per step), 0 per 
 unsigned g_split = 0u;  // CTAs per block pair: 0 automatic (the tuned choice, else by the SM count), else 1, 2, 4
 unsigned g_pairs_per_cta = 0u; // block pairs a CTA takes at a time: 0 automatic, 1, or 2
 unsigned g_variant = 0u; // pivot-block factor: 0 Gram + Cholesky, 1 QR (-DUSE_QR), 2 QR + Drmac (-DUSE_DRMAC)
+int g_batch_mode = -1;   // batched form: -1 the tuned choice (else per step), 0 one launch per step, 1 per sweep
+unsigned g_batch_cap = 0u; // nonzero: the batched form stops after this many sweeps (the autotuner's runs)
+// the batched autotuner's choices, by the batch's sorted (nrow, ncol, signature) list
+std::map<std::vector<unsigned>, std::pair<unsigned, int>> g_batch_tuned; // (pairs per CTA, mode)
 
 // the autotuner's choices, by (routine, nrow, ncol, nplus)
 struct TuneKey {
@@ -430,6 +434,25 @@ int batch_table(DevCtx &ctx, const unsigned n1, const uint16_t *&dtab, unsigned 
   return 0;
 }
 
+// the autotuner's key of a batch: its matrices' (nrow, ncol, signature
+// kind) sorted, so that the same shapes in any order share their choice
+std::vector<unsigned> batch_key(const unsigned nmat, const unsigned *const nrow, const unsigned *const ncol,
+                                const unsigned *const nplus)
+{
+  std::vector<unsigned> k;
+  k.reserve(3u * nmat);
+  std::vector<std::tuple<unsigned, unsigned, unsigned>> v(nmat);
+  for (unsigned b = 0u; b < nmat; ++b)
+    v[b] = std::make_tuple(nrow[b], ncol[b], nplus[b] ? ((nplus[b] < ncol[b]) ? 1u : 2u) : 0u);
+  std::sort(v.begin(), v.end());
+  for (const auto &t : v) {
+    k.push_back(std::get<0>(t));
+    k.push_back(std::get<1>(t));
+    k.push_back(std::get<2>(t));
+  }
+  return k;
+}
+
 // The batched form: nmat independent decompositions, each exactly as
 // run_sweeps_core would do it alone (same steps, same per-pair code, same
 // convergence test), run together: one launch per outer step index for all
@@ -447,6 +470,7 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
     return r;
   if (!ctx->batch_ready) {
     GJX_CUDA(gjx::batch_configure(), "batch_configure");
+    GJX_CUDA(gjx::flow_configure(), "flow_configure");
     GJX_CUDA(cudaStreamCreateWithFlags(&ctx->batch_stream, cudaStreamNonBlocking), "batch stream");
     GJX_CUDA(cudaEventCreateWithFlags(&ctx->batch_ev, cudaEventDisableTiming), "batch event");
     ctx->batch_ready = true;
@@ -563,6 +587,102 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
   int dev = 0, sms = 148;
   GJX_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
   GJX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+  unsigned width = (g_pairs_per_cta == 1u) ? 1u : 2u;
+  int mode = g_batch_mode;
+  {
+    const auto t = g_batch_tuned.find(batch_key(nmat, nrow, ncol, nplus));
+    if (t != g_batch_tuned.end()) {
+      if (!g_pairs_per_cta)
+        width = t->second.first;
+      if (mode < 0)
+        mode = t->second.second;
+    }
+  }
+  const unsigned cap = g_batch_cap ? g_batch_cap : gjx::kNSweep;
+  if (mode == 1) { // one launch per sweep (the dataflow form)
+    std::vector<uint32_t> fitems;
+    std::vector<uint16_t> fsteps;
+    std::vector<unsigned> vofs(nmat, 0u);
+    unsigned nver = 0u;
+    for (unsigned b = 0u; b < nmat; ++b)
+      if (ok[b]) {
+        vofs[b] = nver;
+        nver += 2u * mats[b].p.pairs;
+      }
+    for (unsigned st1 = 0u; st1 < max_steps; ++st1)
+      for (unsigned b : order)
+        if (st1 < mats[b].steps1)
+          for (unsigned q = 0u; q < mats[b].p.pairs; ++q) {
+            fitems.push_back((b << 16u) | q);
+            fsteps.push_back((uint16_t)st1);
+          }
+    const size_t f_items = 0u, f_steps = up(f_items + fitems.size() * 4u), f_ver = up(f_steps + fsteps.size() * 2u),
+                 f_vofs = up(f_ver + (size_t)nver * 4u), ftotal = up(f_vofs + (size_t)nmat * 4u);
+    char *fmem = nullptr;
+    GJX_CUDA(cudaMalloc(&fmem, ftotal), "cudaMalloc(batch flow)");
+    Free free_fmem{fmem};
+    auto *d_fitems = reinterpret_cast<uint32_t *>(fmem + f_items);
+    auto *d_fsteps = reinterpret_cast<uint16_t *>(fmem + f_steps);
+    auto *d_ver = reinterpret_cast<unsigned *>(fmem + f_ver);
+    auto *d_vofs = reinterpret_cast<unsigned *>(fmem + f_vofs);
+    GJX_CUDA(cudaMemcpyAsync(d_fitems, fitems.data(), fitems.size() * 4u, cudaMemcpyHostToDevice, st), "upload");
+    GJX_CUDA(cudaMemcpyAsync(d_fsteps, fsteps.data(), fsteps.size() * 2u, cudaMemcpyHostToDevice, st), "upload");
+    GJX_CUDA(cudaMemcpyAsync(d_vofs, vofs.data(), nmat * 4u, cudaMemcpyHostToDevice, st), "upload");
+    GJX_CUDA(cudaMemsetAsync(d_ver, 0, (size_t)nver * 4u, st), "clear block counts");
+    constexpr unsigned kSweeps = 4u; // sweeps per graph
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    GJX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t ce = cudaSuccess;
+    const gjx::BatchFlow bf{d_mats, d_fitems, d_fsteps, (unsigned)fitems.size(), d_q, d_done, d_ver, d_vofs, d_err};
+    const gjx::BatchSweep sw{d_mats, d_ks, d_cvg, d_done, d_swp, d_gs, d_gb, d_q, d_act, nmat};
+    const unsigned ctas = std::min<unsigned>((unsigned)sms, (unsigned)fitems.size());
+    for (unsigned k = 0u; k < kSweeps && ce == cudaSuccess; ++k) {
+      ce = gjx::launch_batch_flow(cdsort, full, width, bf, ctas, st);
+      if (ce == cudaSuccess)
+        ce = cudaMemsetAsync(d_act, 0, 4u, st);
+      if (ce == cudaSuccess)
+        ce = gjx::launch_batch_flow_end(sw, d_ver, d_vofs, st);
+    }
+    const cudaError_t ee = cudaStreamEndCapture(st, &graph);
+    GJX_CUDA(ce, "capture of batch sweeps");
+    GJX_CUDA(ee, "end capture");
+    struct Graph {
+      cudaGraph_t g;
+      cudaGraphExec_t *x;
+      ~Graph()
+      {
+        if (*x)
+          (void)cudaGraphExecDestroy(*x);
+        if (g)
+          (void)cudaGraphDestroy(g);
+      }
+    } guard{graph, &exec};
+    GJX_CUDA(cudaGraphInstantiate(&exec, graph, 0ull), "graph instantiate");
+    unsigned active = 0u;
+    int err = 0;
+    for (unsigned k = 0u; k * kSweeps < cap; ++k) {
+      GJX_CUDA(cudaGraphLaunch(exec, st), "graph launch");
+      g_prof.launches += 2u * kSweeps;
+      g_prof.l1_launches += kSweeps;
+      GJX_CUDA(cudaMemcpyAsync(&active, d_act, 4u, cudaMemcpyDeviceToHost, st), "read batch state");
+      GJX_CUDA(cudaMemcpyAsync(&err, d_err, 4u, cudaMemcpyDeviceToHost, st), "read batch state");
+      GJX_CUDA(cudaStreamSynchronize(st), "batch sweeps");
+      if (err) {
+        g_err = "a block-pair kernel timed out waiting for its tile copies or blocks";
+        return GJX_ERR_DEVICE;
+      }
+      if (!active)
+        break;
+    }
+    GJX_CUDA(gjx::launch_batch_initD(d_mats, nmat, d_ok, st), "batch initD");
+    ++g_prof.launches;
+    GJX_CUDA(cudaMemcpyAsync(sweeps, d_swp, nmat * 4u, cudaMemcpyDeviceToHost, st), "read sweeps");
+    GJX_CUDA(cudaMemcpyAsync(glb_s, d_gs, nmat * 8u, cudaMemcpyDeviceToHost, st), "read counts");
+    GJX_CUDA(cudaMemcpyAsync(glb_b, d_gb, nmat * 8u, cudaMemcpyDeviceToHost, st), "read counts");
+    GJX_CUDA(cudaStreamSynchronize(st), "batch end");
+    return 0;
+  }
 
   // kLaunches launches (each followed by its step end), captured once
   constexpr unsigned kLaunches = 8u;
@@ -574,7 +694,7 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
   const gjx::BatchSweep sw{d_mats, d_ks, d_cvg, d_done, d_swp, d_gs, d_gb, d_q, d_act, nmat};
   const unsigned ctas = std::min<unsigned>((unsigned)sms, (unsigned)items.size());
   for (unsigned k = 0u; k < kLaunches && ce == cudaSuccess; ++k) {
-    ce = gjx::launch_batch_step(cdsort, full, (g_pairs_per_cta == 1u) ? 1u : 2u, bs, ctas, st);
+    ce = gjx::launch_batch_step(cdsort, full, width, bs, ctas, st);
     if (ce == cudaSuccess)
       ce = cudaMemsetAsync(d_act, 0, 4u, st); // the count of the last launch is the one read
     if (ce == cudaSuccess)
@@ -596,7 +716,7 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
   } guard{graph, &exec};
   GJX_CUDA(cudaGraphInstantiate(&exec, graph, 0ull), "graph instantiate");
 
-  const unsigned max_replays = (gjx::kNSweep * max_steps + kLaunches - 1u) / kLaunches + 1u;
+  const unsigned max_replays = (cap * max_steps + kLaunches - 1u) / kLaunches + 1u;
   unsigned active = 0u;
   int err = 0;
   for (unsigned k = 0u; k < max_replays; ++k) {
@@ -1175,6 +1295,115 @@ void gjx_set_pairs_per_cta(const unsigned w)
   g_pairs_per_cta = (w == 1u || w == 2u) ? w : 0u;
 }
 
+int gjx_autotune_batched(const unsigned routine, const unsigned nmat, const unsigned *const nrow,
+                         const unsigned *const ncol, const unsigned *const nplus, const unsigned sweeps,
+                         unsigned *const out)
+{
+  if (!nmat || nmat > 65535u || !nrow || !ncol || !nplus || routine >= 16u)
+    return -1;
+  for (unsigned b = 0u; b < nmat; ++b)
+    if (const int r = check_args(routine, nrow[b], ncol[b], nplus[b], reinterpret_cast<const double *>(16), nrow[b],
+                                 reinterpret_cast<const double *>(16), ncol[b], reinterpret_cast<const double *>(16),
+                                 reinterpret_cast<const unsigned *>(16),
+                                 reinterpret_cast<const unsigned long long *>(16),
+                                 reinterpret_cast<const unsigned long long *>(16)))
+      return r;
+  std::lock_guard<std::mutex> lk(g_mtx);
+  if (!g_strat.loaded)
+    return GJX_ERR_NO_STRAT;
+  if (g_variant) {
+    g_err = "the batched form takes the default pivot-block factor (gjx_set_variant(0))";
+    return -1;
+  }
+  const bool full = (routine & GJX_FULL_SVD) != 0u;
+  // seeded random matrices of the batch's shapes, one allocation, kept to refill
+  std::vector<size_t> oG(nmat), oV(nmat), oD(nmat);
+  std::vector<unsigned> ldG(nmat), ldV(nmat);
+  size_t nG = 0u, nV = 0u, nD = 0u;
+  for (unsigned b = 0u; b < nmat; ++b) {
+    ldG[b] = nrow[b] + (nrow[b] & 1u);
+    ldV[b] = ncol[b] + (ncol[b] & 1u);
+    oG[b] = nG;
+    nG += (size_t)ldG[b] * ncol[b];
+    oV[b] = nV;
+    nV += full ? (size_t)ldV[b] * ncol[b] : 0u;
+    oD[b] = nD;
+    nD += ncol[b];
+  }
+  double *mem = nullptr;
+  GJX_CUDA(cudaMalloc(&mem, (2u * nG + nV + nD) * sizeof(double)), "cudaMalloc(batch autotune)");
+  struct Free {
+    double *m;
+    ~Free() { (void)cudaFree(m); }
+  } fm{mem};
+  double *const g0 = mem, *const g = mem + nG, *const v = g + nG, *const d = v + nV;
+  GJX_CUDA(gjx::launch_fill_random(g0, nG, 0x5eedba7cull + nmat, nullptr), "autotune input");
+  std::vector<double *> pG(nmat), pV(nmat), pD(nmat);
+  for (unsigned b = 0u; b < nmat; ++b) {
+    pG[b] = g + oG[b];
+    pV[b] = full ? v + oV[b] : nullptr;
+    pD[b] = d + oD[b];
+  }
+  std::vector<unsigned> swp(nmat);
+  std::vector<unsigned long long> s_(nmat), b_(nmat);
+  std::vector<int> info(nmat);
+  cudaEvent_t e0, e1;
+  GJX_CUDA(cudaEventCreate(&e0), "cudaEventCreate");
+  GJX_CUDA(cudaEventCreate(&e1), "cudaEventCreate");
+  const int saved_mode = g_batch_mode;
+  const unsigned saved_width = g_pairs_per_cta, saved_cap = g_batch_cap;
+  g_batch_cap = sweeps ? sweeps : 1u;
+  float best = 3.0e38f;
+  std::pair<unsigned, int> pick{2u, 0};
+  int rc = 0;
+  for (unsigned width : {2u, 1u}) {
+    for (int mode : {0, 1}) {
+      g_pairs_per_cta = width;
+      g_batch_mode = mode;
+      float ms = 0.0f;
+      for (int rep = 0; rep < 2 && !rc; ++rep) { // the first run warms up
+        if (cudaMemcpyAsync(g, g0, nG * sizeof(double), cudaMemcpyDeviceToDevice, nullptr) != cudaSuccess ||
+            cudaEventRecord(e0, nullptr) != cudaSuccess) {
+          rc = GJX_ERR_CUDA;
+          break;
+        }
+        rc = run_batch(routine, nmat, nrow, ncol, nplus, pG.data(), ldG.data(), pV.data(), ldV.data(), pD.data(),
+                       nullptr, swp.data(), s_.data(), b_.data(), info.data());
+        if (!rc && (cudaEventRecord(e1, nullptr) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                    cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+          rc = GJX_ERR_CUDA;
+      }
+      if (rc)
+        break;
+      if (ms < best) {
+        best = ms;
+        pick = {width, mode};
+      }
+    }
+    if (rc)
+      break;
+  }
+  g_batch_mode = saved_mode;
+  g_pairs_per_cta = saved_width;
+  g_batch_cap = saved_cap;
+  (void)cudaEventDestroy(e0);
+  (void)cudaEventDestroy(e1);
+  if (rc)
+    return rc;
+  g_batch_tuned[batch_key(nmat, nrow, ncol, nplus)] = pick;
+  if (out) {
+    out[0] = pick.first;
+    out[1] = (unsigned)pick.second;
+  }
+  return 0;
+}
+
+void gjx_set_batch_mode(const int mode)
+{
+  std::lock_guard<std::mutex> lk(g_mtx);
+  g_batch_mode = (mode < 0) ? -1 : (mode ? 1 : 0);
+}
+
 int gjx_autotune(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
                  const unsigned sweeps, unsigned *const out)
 {
@@ -1265,6 +1494,7 @@ void gjx_autotune_clear(void)
 {
   std::lock_guard<std::mutex> lk(g_mtx);
   g_tuned.clear();
+  g_batch_tuned.clear();
 }
 
 int gjx_wait_selftest(const long long limit_cycles, const unsigned ctas, int *const timed_out,

@@ -70,7 +70,25 @@ struct BatchSweep {
   unsigned nmat;
 };
 
+// one launch per sweep of a batch (the dataflow form): the items of every
+// matrix's steps, step-major; an item waits for its blocks' previous step
+struct BatchFlow {
+  const BatchMat *mats;
+  const uint32_t *items;  // (matrix << 16) | pair
+  const uint16_t *isteps; // the item's step within the sweep
+  unsigned nitems;
+  unsigned *queue;        // work-queue head (cleared by the sweep end)
+  const uint32_t *done;   // converged or failed matrices (skipped)
+  unsigned *ver;          // per matrix at vofs[b]: per block, the writes of this sweep
+  const unsigned *vofs;
+  int *err;
+};
+
 cudaError_t batch_configure();
+cudaError_t flow_configure();
+cudaError_t launch_batch_flow(bool sort, bool accv, unsigned width, const BatchFlow &b, unsigned ctas,
+                              cudaStream_t s);
+cudaError_t launch_batch_flow_end(const BatchSweep &w, unsigned *ver, const unsigned *vofs, cudaStream_t s);
 cudaError_t launch_fill_random(double *a, size_t n, unsigned long long seed, cudaStream_t s);
 cudaError_t launch_wait_selftest(long long limit, int *timed_out, long long *cycles, unsigned ctas, cudaStream_t s);
 // one launch for a whole sweep (all outer steps), when every cluster of the

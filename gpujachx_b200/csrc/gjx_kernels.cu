@@ -1415,6 +1415,145 @@ __global__ void __launch_bounds__(kThreads, 1) l1_batch_kernel(const __grid_cons
   }
 }
 
+// One launch per sweep of the whole batch (the dataflow form): the CTAs take
+// (matrix, step, pair) items in queue order -- step-major, every matrix's
+// step s before any step s + 1 -- and an item waits until both of its blocks
+// have been written by its matrix's step s - 1 (per-block counts of the
+// sweep, release / acquire, bounded waits).  Steps of different matrices, and
+// the pairs of consecutive steps of one matrix whose blocks are ready,
+// overlap.  An item waits only on items taken earlier, by running CTAs, so
+// the launch needs no co-residency.  Two items go through pair_step2 when
+// neither can depend on the other (different matrices, or the same step).
+template <bool SORT, bool ACCV, unsigned W>
+__global__ void __launch_bounds__(kThreads, 1) l1_batch_flow_kernel(const __grid_constant__ BatchFlow B)
+{
+  extern __shared__ __align__(128) double sm[];
+  __shared__ unsigned item, ok;
+  uint64_t *const bars = reinterpret_cast<uint64_t *>(sm + kOffBar);
+  const unsigned tid = threadIdx.x;
+  // thread 0: wait until item h's blocks are written by its previous step
+  auto ready = [&](const uint32_t e, const unsigned stp) -> bool {
+    const unsigned b = e >> 16u, q = e & 0xffffu;
+    const BatchMat &m = B.mats[b];
+    const size_t pidx = ((size_t)stp * m.p.pairs + q) * 2u;
+    const unsigned *const v = B.ver + B.vofs[b];
+    const unsigned iB = m.p.strat1[pidx], jB = m.p.strat1[pidx + 1u];
+    const long long t0 = clock64();
+    while (ld_acquire(v + iB) < stp || ld_acquire(v + jB) < stp) {
+      if (*(volatile int *)B.err)
+        return false;
+      if (clock64() - t0 > kWaitLimit) {
+        atomicOr(B.err, kErrWaitTimeout);
+        return false;
+      }
+      __nanosleep(64);
+    }
+    return true;
+  };
+  auto written = [&](const uint32_t e, const unsigned stp) { // thread 0, after the pair's stores completed
+    const unsigned b = e >> 16u, q = e & 0xffffu;
+    const BatchMat &m = B.mats[b];
+    const size_t pidx = ((size_t)stp * m.p.pairs + q) * 2u;
+    unsigned *const v = B.ver + B.vofs[b];
+    __threadfence();
+    atomicAdd(v + m.p.strat1[pidx], 1u);
+    atomicAdd(v + m.p.strat1[pidx + 1u], 1u);
+  };
+  auto inval = [&]() {
+    __syncthreads();
+    if (tid == 0u)
+      for (unsigned k = 0u; k < 8u; ++k)
+        mbar_inval(&bars[k]);
+    __syncthreads();
+  };
+  for (;;) {
+    if (tid == 0u)
+      item = atomicAdd(B.queue, W);
+    __syncthreads();
+    const unsigned it = item;
+    const bool stop = (it >= B.nitems) || (*(volatile int *)B.err != 0);
+    __syncthreads();
+    if (stop)
+      break;
+    uint32_t e[2] = {B.items[it], 0u};
+    unsigned st[2] = {B.isteps[it], 0u};
+    bool live[2] = {!B.done[e[0] >> 16u], false};
+    if (W == 2u && it + 1u < B.nitems) {
+      e[1] = B.items[it + 1u];
+      st[1] = B.isteps[it + 1u];
+      live[1] = !B.done[e[1] >> 16u];
+    }
+    const unsigned b0 = e[0] >> 16u, b1 = e[1] >> 16u;
+    const bool both = live[0] && live[1] && (b0 != b1 || st[0] == st[1]) &&
+                      B.mats[b0].p.strat0 == B.mats[b1].p.strat0;
+    if (both) {
+      if (tid == 0u)
+        ok = ready(e[0], st[0]) && ready(e[1], st[1]);
+      __syncthreads();
+      if (!ok)
+        break;
+      asm volatile("fence.proxy.async;" ::: "memory"); // the copies below read what other SMs wrote
+      const BatchMat &ma = B.mats[b0], &mb = B.mats[b1];
+      pair_step2<SORT, ACCV>(ma.p, st[0], e[0] & 0xffffu, mb.p, st[1], e[1] & 0xffffu, sm);
+      __threadfence();
+      __syncthreads();
+      if (tid == 0u) {
+        written(e[0], st[0]);
+        written(e[1], st[1]);
+      }
+      inval();
+      continue;
+    }
+    bool go = true;
+    for (unsigned h = 0u; h < 2u && go; ++h) {
+      if (!live[h])
+        continue;
+      if (tid == 0u)
+        ok = ready(e[h], st[h]);
+      __syncthreads();
+      if (!ok) {
+        go = false;
+        break;
+      }
+      asm volatile("fence.proxy.async;" ::: "memory");
+      const BatchMat &m = B.mats[e[h] >> 16u];
+      pair_step<SORT, ACCV, 1u>(m.p, st[h], e[h] & 0xffffu, 0u, sm);
+      __threadfence();
+      __syncthreads();
+      if (tid == 0u)
+        written(e[h], st[h]);
+      inval();
+    }
+    if (!go)
+      break;
+  }
+}
+
+// after a sweep of the dataflow form: per matrix still sweeping, the sweep's
+// counter folded into its totals and the convergence test (no big rotation,
+// or the sweep cap); its block counts and the queue cleared for the next
+__global__ void batch_flow_end_kernel(const BatchSweep S, unsigned *const ver, const unsigned *const vofs)
+{
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0u)
+    S.queue[0] = 0u;
+  if (i >= S.nmat || S.done[i])
+    return;
+  const unsigned n1 = S.mats[i].p.pairs * 2u;
+  for (unsigned k = 0u; k < n1; ++k)
+    ver[vofs[i] + k] = 0u;
+  const unsigned long long c = S.cvg[i];
+  S.cvg[i] = 0ull;
+  const unsigned small = (unsigned)c, big = (unsigned)(c >> 32u);
+  S.glb_s[i] += small;
+  S.glb_b[i] += big;
+  const unsigned sw = ++S.sweeps[i];
+  if (!big || sw >= kNSweep)
+    S.done[i] = 1u;
+  else
+    atomicAdd(S.active, 1u);
+}
+
 // after a launch of the batch: one step more for every active matrix; at the
 // end of its sweep, its totals and the convergence test (no big rotation in
 // the sweep, or the sweep cap); the work queue cleared for the next launch
@@ -1705,6 +1844,56 @@ cudaError_t launch_batch_step(const bool sort, const bool accv, const unsigned w
     batch_launch<false, true>(width, b, ctas, s);
   else
     batch_launch<false, false>(width, b, ctas, s);
+  return cudaGetLastError();
+}
+
+template <bool S, bool A> static cudaError_t set_smem_flow()
+{
+  cudaError_t e = cudaFuncSetAttribute(l1_batch_flow_kernel<S, A, 1u>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)l1_smem_bytes());
+  if (e != cudaSuccess)
+    return e;
+  return cudaFuncSetAttribute(l1_batch_flow_kernel<S, A, 2u>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)batch2_smem_bytes());
+}
+
+cudaError_t flow_configure()
+{
+  cudaError_t e;
+  if ((e = set_smem_flow<false, false>()) || (e = set_smem_flow<false, true>()) || (e = set_smem_flow<true, false>()) ||
+      (e = set_smem_flow<true, true>()))
+    return e;
+  return cudaSuccess;
+}
+
+template <bool S, bool A>
+static void flow_launch(const unsigned width, const BatchFlow &b, const unsigned ctas, cudaStream_t s)
+{
+  if (width == 2u)
+    l1_batch_flow_kernel<S, A, 2u><<<ctas, kThreads, batch2_smem_bytes(), s>>>(b);
+  else
+    l1_batch_flow_kernel<S, A, 1u><<<ctas, kThreads, l1_smem_bytes(), s>>>(b);
+}
+
+cudaError_t launch_batch_flow(const bool sort, const bool accv, const unsigned width, const BatchFlow &b,
+                              const unsigned ctas, cudaStream_t s)
+{
+  if (sort) {
+    if (accv)
+      flow_launch<true, true>(width, b, ctas, s);
+    else
+      flow_launch<true, false>(width, b, ctas, s);
+  }
+  else if (accv)
+    flow_launch<false, true>(width, b, ctas, s);
+  else
+    flow_launch<false, false>(width, b, ctas, s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_flow_end(const BatchSweep &w, unsigned *ver, const unsigned *vofs, cudaStream_t s)
+{
+  batch_flow_end_kernel<<<(w.nmat + 255u) / 256u, 256u, 0, s>>>(w, ver, vofs);
   return cudaGetLastError();
 }
 

@@ -139,6 +139,25 @@ void gjx_set_variant(unsigned v);
 int gjx_autotune(unsigned routine, unsigned nrow, unsigned ncol, unsigned nplus, unsigned sweeps, unsigned *out);
 void gjx_autotune_clear(void);
 
+/* The batched form's launches: -1 (default) the tuned choice
+ * (gjx_autotune_batched), else one launch per outer step index; 0 one launch
+ * per outer step index for the whole batch (every active matrix advances one
+ * step), replayed from a CUDA graph; 1 one launch per sweep of the whole
+ * batch, in which a CTA takes (matrix, step, pair) items in step order and
+ * starts one as soon as its two blocks have been written by its matrix's
+ * previous step.  The results are the same bits either way. */
+void gjx_set_batch_mode(int mode);
+
+/* Autotuner of the batched form: times block pairs per CTA (2, 1) x launch
+ * mode (per step, per sweep) on seeded random matrices of the batch's shapes
+ * (nrow[b] x ncol[b], the signature kind of nplus[b]), `sweeps` sweeps each
+ * (0: 1), and uses the fastest in later gjx_hypJacL2_batched calls on a
+ * batch of the same shapes (in any order) unless gjx_set_pairs_per_cta /
+ * gjx_set_batch_mode fix them.  out[2] = {pairs per CTA, mode}.  0 or an
+ * error code. */
+int gjx_autotune_batched(unsigned routine, unsigned nmat, const unsigned *nrow, const unsigned *ncol,
+                         const unsigned *nplus, unsigned sweeps, unsigned *out);
+
 /* Failure-path self test of the bounded waits every kernel here uses (an
  * mbarrier or flag that never completes makes the kernel give up after a
  * cycle limit and report, instead of hanging): ctas CTAs each wait on an

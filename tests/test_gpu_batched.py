@@ -29,12 +29,14 @@ CASES = [(64, 64, 64), (128, 128, 64), (192, 192, 0), (256, 256, 256), (320, 320
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("mode", [0, 1])
 @pytest.mark.parametrize("width", [2, 1])
 @pytest.mark.parametrize("alg", [11, 9, 3, 1])
-def test_batched_equals_single(built, alg, width):
+def test_batched_equals_single(built, alg, width, mode):
     import torch
     import gpujachx_b200 as g
     g.lib().gjx_set_pairs_per_cta(width)   # 2: two block pairs per CTA, from different matrices too
+    g.lib().gjx_set_batch_mode(mode)       # 0: one launch per step index, 1: one launch per sweep
     g.init_strats(None, "cycwor", 32, "cycwor", 4)   # the family; each matrix takes its own n1 table
     full = bool(alg & 2)
     mats = []
@@ -46,6 +48,7 @@ def test_batched_equals_single(built, alg, width):
     res = g.hypJacL2_batched(alg, [b[0] for b in batch], [p for _, p in mats], Vs=[b[1] for b in batch] if full else None,
                              Ds=[b[2] for b in batch])
     g.lib().gjx_set_pairs_per_cta(0)
+    g.lib().gjx_set_batch_mode(-1)
     assert res.info == [0] * len(mats)
     for k, (G, p) in enumerate(mats):
         n = G.shape[1]
@@ -76,3 +79,29 @@ def test_batched_bad_matrix_is_reported(built):
     ref = _dev(G1, True)
     r = g.hypJacL2_dev(11, ref[0], 64, ref[1], ref[2])
     assert res.sweeps[0] == r[1] and np.array_equal(_bits(good[0]), _bits(ref[0]))
+
+
+@pytest.mark.gpu
+def test_batch_autotuner_picks_and_keeps_bits(built):
+    """gjx_autotune_batched times (pairs per CTA) x (per-step / per-sweep
+    launches) on random matrices of the batch's shapes; the batch run after it
+    (with the tuned choice) still gives every matrix the single call's bits."""
+    import torch
+    import gpujachx_b200 as g
+    shapes = [(128, 128, 128), (256, 256, 128), (192, 192, 0), (320, 320, 320), (128, 64, 64)]
+    g.init_strats(None, "cycwor", 32, "cycwor", 4)
+    pick = g.autotune_batched(11, [m for m, _, _ in shapes], [n for _, n, _ in shapes], [p for _, _, p in shapes])
+    assert pick["pairs_per_cta"] in (1, 2) and pick["mode"] in (0, 1)
+    mats = [synth.make("svd_synth", m, n, 7000 + k, smin=1e-6) if m == n else synth.make("graded", m, n, 7000 + k)
+            for k, (m, n, _) in enumerate(shapes)]
+    batch = [_dev(G, True) for G in mats]
+    res = g.hypJacL2_batched(11, [b[0] for b in batch], [p for _, _, p in shapes], Vs=[b[1] for b in batch],
+                             Ds=[b[2] for b in batch])
+    g.lib().gjx_autotune_clear()
+    for k, (G, (m, n, p)) in enumerate(zip(mats, shapes)):
+        g.init_strats(None, "cycwor", 32, "cycwor", n // 16)
+        dG, dV, dD = _dev(G, True)
+        ret, sw, rs, rb = g.hypJacL2_dev(11, dG, p, dV, dD)
+        torch.cuda.synchronize()
+        assert (res.sweeps[k], res.rot_s[k], res.rot_b[k]) == (sw, rs, rb)
+        assert np.array_equal(_bits(batch[k][0]), _bits(dG)) and np.array_equal(_bits(batch[k][1]), _bits(dV))
