@@ -265,6 +265,13 @@ __device__ __forceinline__ Rot inner_rot(const double Dp, const double Dq, const
   return r;
 }
 
+// a named barrier for the nthreads threads of a warp group (id 0 with all the
+// CTA's threads is __syncthreads)
+__device__ __forceinline__ void bar_sync(const unsigned id, const unsigned nthreads)
+{
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // mbarrier + bulk-copy (TMA engine) helpers, with bounded waits
 // ---------------------------------------------------------------------------

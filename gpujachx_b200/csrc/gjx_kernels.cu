@@ -350,12 +350,6 @@ __device__ __forceinline__ void chol_pivot(double *const R, const unsigned j, co
     E32(R, j, j) = sq;
 }
 
-// a named barrier for the nthreads threads of a warp group (id 0 with all the
-// CTA's threads is __syncthreads)
-__device__ __forceinline__ void bar_sync(const unsigned id, const unsigned nthreads)
-{
-  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
-}
 
 // by a group of NW warps (thread gt of the group, named barrier bar): the
 // group's warp 0 pivots, warps 1..NW-1 update the trailing columns

@@ -95,10 +95,13 @@ struct Params {
   long long *clk; // block 0 of sp_pair_kernel: clock64 at the phase ends (gjx_split_phase_cycles)
 };
 
-// ---- the update's B operand in global memory: 8 digit planes (K-major,
-// 64 x 64 bytes each, core matrices of 8 rows x 16 bytes, LBO 128, SBO 512)
-// then the 64 column exponents h_j
-constexpr uint32_t kBPlane = 4096u;
+// ---- the update's B operand in global memory: for each half of the output
+// columns (32 each) the 7 digit planes side by side (K-major, 32 x 64 bytes
+// each, core matrices of 8 rows x 16 bytes, LBO 128, SBO 512), then the 64
+// column exponents h_j
+constexpr uint32_t kBHalfPlane = 2048u;
+constexpr uint32_t kBHalf = kDig * kBHalfPlane; // 14336
+constexpr uint32_t kBPlane = 4096u;              // both halves of a digit
 constexpr uint32_t kBopBytes = kDig * kBPlane + 256u;
 
 // ---------------------------------------------------------------------------
@@ -456,10 +459,10 @@ __device__ void inner64(double *const R, double *const Vl, const uint8_t *const 
   }
 }
 
-// the update's B operand diag(2^e_k) V_loc of one matrix: 8 digit planes
-// (K-major, n = output column j, k = pair column) and the exponents h_j,
-// written to global memory.  Thread (j = tid / 4, kg = tid % 4) takes
-// k = 16 kg .. 16 kg + 15 of column j.
+// the update's B operand diag(2^e_k) V_loc of one matrix: its digit planes
+// (K-major, n = output column j, k = pair column; the columns of each half
+// apart) and the exponents h_j, written to global memory.  Thread
+// (j = tid / 4, kg = tid % 4) takes k = 16 kg .. 16 kg + 15 of column j.
 __device__ void bop_write(const double *const Vl, const int *const e, uint8_t *const out)
 {
   const unsigned tid = threadIdx.x, j = tid >> 2, kg = tid & 3u;
@@ -483,7 +486,8 @@ __device__ void bop_write(const double *const Vl, const int *const e, uint8_t *c
   digits16(w, pl);
 #pragma unroll
   for (unsigned t = 0u; t < kDig; ++t)
-    *reinterpret_cast<uint4 *>(out + t * kBPlane + (j >> 3) * 512u + kg * 128u + (j & 7u) * 16u) = pl[t];
+    *reinterpret_cast<uint4 *>(out + (j >> 5) * kBHalf + t * kBHalfPlane + ((j & 31u) >> 3) * 512u + kg * 128u +
+                               (j & 7u) * 16u) = pl[t];
   if (kg == 0u)
     reinterpret_cast<int *>(out + kDig * kBPlane)[j] = h;
 }
@@ -783,42 +787,41 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
 // and V, A the FP64 tile, B = V_loc (its digit planes diag(2^e) V_loc from
 // sp_pair_kernel); C replaces A.  A persistent grid: CTA c takes a
 // contiguous run of the items (pair, tile), tiles of a pair in order (G's,
-// then V's), so its B operand changes rarely.  Per item: the FP64 tile
-// (TMA, two items ahead, double-buffered) is cut into the 8 digit planes of
-// A, 72 MMAs of 128 x 64 x 32 into 8 int32 accumulators, then each thread
-// recombines its row's outputs (int64 group sums, two conversions) and
-// stores them straight to global memory (a warp writes 256 contiguous bytes
-// per column), folding their magnitudes into the columns' maxima.
+// then V's), so its B operand changes rarely.  Two warp groups work on
+// consecutive items at once:
+//   warps 4-7 (cutters) wait for the FP64 tile of item i (TMA, two items
+//     ahead, double-buffered), cut it into the 7 digit planes of A, and one
+//     lane issues the MMAs: for each half of the output columns and each
+//     digit t of A, one 128 x 32 (7 - t) x 32 MMA per K half against the B
+//     planes t..6 side by side -- 28 MMAs, the half's 7 int32 group sums in
+//     224 TMEM columns;
+//   warps 0-3 (epilogue) take each half as soon as its MMAs complete, sum its
+//     groups in int64, convert exactly, scale, store the row straight to
+//     global memory (a warp writes 256 contiguous bytes per column) and fold
+//     the magnitudes into the columns' maxima, then free the half's TMEM.
+// So the cutting of item i + 1 and the MMAs of one half overlap the
+// epilogue of the other.  Every wait is bounded; on a timeout the kernel
+// sets the error word and both groups leave.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kUStage = 128u * 64u * 8u;                  // FP64 tile, column c at c * 128 doubles
 constexpr uint32_t kUAPlane = 8192u;                            // 128 x 64 bytes, K-major, LBO 128, SBO 512
 constexpr uint32_t kOffUStage = 0u;                             // two tiles
 constexpr uint32_t kOffUA = 2u * kUStage;                       // 131072
 constexpr uint32_t kOffUB = kOffUA + kDig * kUAPlane;           // 188416
-constexpr uint32_t kOffUScale = kOffUB + kBopBytes;             // 64 double cut factors, 64 double output
-                                                                // scales, [4][64] uint maxima of the row quarters
-constexpr uint32_t kOffUBar = kOffUScale + 2048u;               // [0, 1] tiles, [2] B operand, [3] MMAs
-constexpr uint32_t kOffUTmem = kOffUBar + 32u;
-constexpr uint32_t kUpdSmem = kOffUTmem + 16u;
+constexpr uint32_t kOffUFk = kOffUB + kBopBytes;                // 64 double: cut factors of A's columns
+constexpr uint32_t kOffUFo = kOffUFk + 512u;                    // [2][64] double: output scales, by item parity
+constexpr uint32_t kOffUCm = kOffUFo + 1024u;                   // [4][64] uint: maxima of the row quarters
+constexpr uint32_t kOffUBar = kOffUCm + 1024u;                  // 10 mbarriers
+constexpr uint32_t kOffUTmem = kOffUBar + 80u;
+constexpr uint32_t kOffUFlag = kOffUTmem + 16u;
+constexpr uint32_t kUpdSmem = kOffUFlag + 16u;
 static_assert(kUpdSmem <= 227u * 1024u, "shared memory of sp_update_kernel");
-
-// int64 t (|t| < 2^51) as a double, exactly: the bits of 1.5 * 2^52 + t minus 1.5 * 2^52
-__device__ __forceinline__ double exact_ll(const long long t)
-{
-  return __longlong_as_double(t + 0x4338000000000000ll) - 0x1.8p+52;
-}
-
-// sum_g 2^-8g S_g (g = 0..6) in FP64: T0 = S0 2^8 + S1, T1 = S2 2^8 + S3,
-// T2 = S4 2^16 + S5 2^8 + S6 are exact int64 (below 2^48) and convert exactly;
-// two roundings
-__device__ __forceinline__ double recombine_u(const int s0, const int s1, const int s2, const int s3, const int s4,
-                                             const int s5, const int s6)
-{
-  const long long t0 = (long long)s0 * 256ll + (long long)s1;
-  const long long t1 = (long long)s2 * 256ll + (long long)s3;
-  const long long t2 = (long long)s4 * 65536ll + (long long)s5 * 256ll + (long long)s6;
-  return __fma_rn(exact_ll(t0), 0x1.0p-8, __fma_rn(exact_ll(t1), 0x1.0p-24, exact_ll(t2) * 0x1.0p-48));
-}
+// mbarriers
+constexpr unsigned kBarFull = 0u;  // [2] FP64 tiles (TMA bytes)
+constexpr unsigned kBarB = 2u;     // B operand (bulk copy bytes)
+constexpr unsigned kBarMma = 3u;   // [2] the MMAs of a half (tcgen05.commit)
+constexpr unsigned kBarFree = 5u;  // [2] a half's TMEM drained (4 epilogue warps)
+constexpr unsigned kBarMeta = 7u;  // [2] an item's output scales written (cutters), by item parity
 
 struct Item {
   unsigned pair, iBlk, jBlk, row0, rows, key;
@@ -849,6 +852,57 @@ __device__ __forceinline__ void load_tile(const Params &P, const Item &it, unsig
   tma_load_2d(dst + kUStage / 2u, tm, (int)it.row0, (int)(it.jBlk * kBW), bar);
 }
 
+// int64 t (|t| < 2^51) as a double, exactly: the bits of 1.5 * 2^52 + t minus 1.5 * 2^52
+__device__ __forceinline__ double exact_ll(const long long t)
+{
+  return __longlong_as_double(t + 0x4338000000000000ll) - 0x1.8p+52;
+}
+
+// sum_g 2^-8g S_g (g = 0..6) in FP64: T0 = S0 2^8 + S1, T1 = S2 2^8 + S3,
+// T2 = S4 2^16 + S5 2^8 + S6 are exact int64 (below 2^48) and convert exactly;
+// two roundings
+__device__ __forceinline__ double recombine_u(const int s0, const int s1, const int s2, const int s3, const int s4,
+                                             const int s5, const int s6)
+{
+  const long long t0 = (long long)s0 * 256ll + (long long)s1;
+  const long long t1 = (long long)s2 * 256ll + (long long)s3;
+  const long long t2 = (long long)s4 * 65536ll + (long long)s5 * 256ll + (long long)s6;
+  return __fma_rn(exact_ll(t0), 0x1.0p-8, __fma_rn(exact_ll(t1), 0x1.0p-24, exact_ll(t2) * 0x1.0p-48));
+}
+
+// a bounded wait that gives up at once when the other group has aborted
+__device__ __forceinline__ bool wait_or_abort(uint64_t *bar, const uint32_t parity, volatile int *abort_flag)
+{
+  if (mbar_try_wait(bar, parity))
+    return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (*abort_flag || clock64() - t0 > kWait)
+      return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// named barrier id of n threads that also ORs their predicates: the same
+// answer in every participating thread
+__device__ __forceinline__ bool bar_or(const unsigned id, const unsigned n, const bool pred)
+{
+  uint32_t r;
+  asm volatile("{\n\t.reg .pred p, q;\n\t"
+               "setp.ne.u32 p, %1, 0;\n\t"
+               "barrier.cta.red.or.pred q, %2, %3, p;\n\t"
+               "selp.u32 %0, 1, 0, q;\n\t}"
+               : "=r"(r)
+               : "r"((uint32_t)pred), "r"(id), "r"(n)
+               : "memory");
+  return r != 0u;
+}
+
 template <bool ACCV>
 __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_constant__ Params P)
 {
@@ -860,14 +914,22 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
   const unsigned it1 = it0 + per + (blockIdx.x < extra ? 1u : 0u);
   uint64_t *const bar = reinterpret_cast<uint64_t *>(sm + kOffUBar);
   uint32_t *const tmem_holder = reinterpret_cast<uint32_t *>(sm + kOffUTmem);
-  double *const fk = reinterpret_cast<double *>(sm + kOffUScale);        // 2^(54 - e_k) of A's columns
-  double *const fo = fk + 64;                                             // 2^(h_j - 12) of C's columns
-  uint32_t *const cm = reinterpret_cast<uint32_t *>(sm + kOffUScale + 1024u); // [row quarter][column]
+  volatile int *const abort_flag = reinterpret_cast<volatile int *>(sm + kOffUFlag);
+  double *const fk = reinterpret_cast<double *>(sm + kOffUFk);
+  double *const fo = reinterpret_cast<double *>(sm + kOffUFo);
+  uint32_t *const cm = reinterpret_cast<uint32_t *>(sm + kOffUCm);
   const int *const hcol = reinterpret_cast<const int *>(sm + kOffUB + kDig * kBPlane);
 
   if (tid == 0u) {
-    for (unsigned i = 0u; i < 4u; ++i)
+    for (unsigned i = 0u; i < 3u; ++i)
       mbar_init(&bar[i], 1u);
+    mbar_init(&bar[kBarMma], 1u);
+    mbar_init(&bar[kBarMma + 1u], 1u);
+    mbar_init(&bar[kBarFree], 4u);
+    mbar_init(&bar[kBarFree + 1u], 4u);
+    mbar_init(&bar[kBarMeta], 1u);
+    mbar_init(&bar[kBarMeta + 1u], 1u);
+    *abort_flag = 0;
     mbar_fence_init();
   }
   if (warp == 0u)
@@ -876,158 +938,167 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
   tc_fence_after();
   const uint32_t tmem = *tmem_holder;
   const uint32_t sbase = smem_u32(sm);
-  if (tid == 0u)
-    for (unsigned k = it0; k < it1 && k < it0 + 2u; ++k)
-      load_tile(P, item_of(P, k), sm + kOffUStage + (k - it0) * kUStage, &bar[k - it0]);
 
-  unsigned key = ~0u, nb = 0u; // the B operand held, and how many were loaded
-  bool failed = false;
-  // the next item's column maxima, loaded one item ahead (threads 0..63)
-  auto col_word = [&](const Item &x) -> uint32_t {
-    const unsigned gc = (tid < kBW) ? x.iBlk * kBW + tid : x.jBlk * kBW + tid - kBW;
-    return (x.isV ? P.cmaxV : P.cmaxG)[P.parity * P.ncol + gc];
-  };
-  uint32_t next_cmax = (tid < 64u && it0 < it1) ? col_word(item_of(P, it0)) : 0u;
-  for (unsigned k = it0, n = 0u; k < it1; ++k, ++n) {
-    const Item it = item_of(P, k);
-    const unsigned buf = n & 1u;
-    uint32_t *const cmax = it.isV ? P.cmaxV : P.cmaxG;
-    if (tid < 64u)
-      fk[tid] = cut_factor(col_exp(next_cmax));
-    const bool rec = blockIdx.x == 0u && tid == 0u;
-    long long c0 = rec ? clock64() : 0;
-    const bool newb = it.key != key;
-    if (newb && tid == 0u) { // the previous item's MMAs are complete: B is free
-      mbar_arrive_expect_tx(&bar[2], kBopBytes);
-      bulk_g2s(sm + kOffUB, P.bop + ((size_t)it.pair * (ACCV ? 2u : 1u) + (it.isV ? 1u : 0u)) * kBopBytes,
-               kBopBytes, &bar[2]);
-    }
-    __syncthreads();
-    int bad = !mbar_wait_bounded(&bar[buf], (n >> 1) & 1u, kWait);
-    if (newb && !mbar_wait_bounded(&bar[2], nb & 1u, kWait))
-      bad = 1;
-    if (__syncthreads_or(bad)) {
-      failed = true;
-      break;
-    }
-    if (newb) {
-      key = it.key;
-      ++nb;
-      if (tid < 64u)
-        fo[tid] = p2(hcol[tid] - 12);
-    }
-    long long c1 = rec ? clock64() : 0;
-    // cut the tile into the digit planes of A: row r, pair columns 16 kg .. 16 kg + 15
-    {
-      const double *const st = reinterpret_cast<const double *>(sm + kOffUStage + buf * kUStage);
-      const unsigned r = tid & 127u;
+  if (warp >= 4u) {
+    // ------------------------------- cutters -------------------------------
+    const unsigned ct = tid - 128u; // 0..127: row ct of the tile
+    const bool lead = ct == 0u;
+    if (lead)
+      for (unsigned k = it0; k < it1 && k < it0 + 2u; ++k)
+        load_tile(P, item_of(P, k), sm + kOffUStage + (k - it0) * kUStage, &bar[kBarFull + (k - it0)]);
+    auto col_word = [&](const Item &x) -> uint32_t {
+      const unsigned gc = (ct < kBW) ? x.iBlk * kBW + ct : x.jBlk * kBW + ct - kBW;
+      return (x.isV ? P.cmaxV : P.cmaxG)[P.parity * P.ncol + gc];
+    };
+    uint32_t next_cmax = (ct < 64u && it0 < it1) ? col_word(item_of(P, it0)) : 0u;
+    unsigned key = ~0u, nb = 0u;
+    for (unsigned k = it0, n = 0u; k < it1; ++k, ++n) {
+      const Item it = item_of(P, k);
+      const unsigned buf = n & 1u;
+      bool ok = true;
+      // the previous item's MMAs are complete: A and B are free
+      if (n > 0u)
+        ok = wait_or_abort(&bar[kBarMma + 1u], (n - 1u) & 1u, abort_flag);
+      const bool newb = it.key != key;
+      if (ok && newb && lead) {
+        mbar_arrive_expect_tx(&bar[kBarB], kBopBytes);
+        bulk_g2s(sm + kOffUB, P.bop + ((size_t)it.pair * (ACCV ? 2u : 1u) + (it.isV ? 1u : 0u)) * kBopBytes,
+                 kBopBytes, &bar[kBarB]);
+      }
+      if (ct < 64u)
+        fk[ct] = cut_factor(col_exp(next_cmax));
+      if (ok && newb)
+        ok = wait_or_abort(&bar[kBarB], nb & 1u, abort_flag);
+      if (ok)
+        ok = wait_or_abort(&bar[kBarFull + buf], (n >> 1) & 1u, abort_flag);
+      if (newb) {
+        key = it.key;
+        ++nb;
+      }
+      if (ct < 64u) // this item's output scales, for the epilogue
+        fo[buf * 64u + ct] = p2(hcol[ct] - 12);
+      // fk and fo written, every cutter's waits done; one decision for all
+      if (bar_or(1u, 128u, !ok || *abort_flag)) {
+        *abort_flag = 1;
+        break;
+      }
+      if (lead)
+        mbar_arrive(&bar[kBarMeta + buf]);
+      // the tile's rows into the digit planes of A: row ct, pair columns 16 kg .. 16 kg + 15
+      {
+        const double *const st = reinterpret_cast<const double *>(sm + kOffUStage + buf * kUStage);
 #pragma unroll 1
-      for (unsigned kg = tid >> 7; kg < 4u; kg += 2u) {
-        long long w[16];
+        for (unsigned kg = 0u; kg < 4u; ++kg) {
+          long long w[16];
 #pragma unroll
-        for (unsigned i = 0u; i < 16u; ++i) {
-          const unsigned c = 16u * kg + i;
-          w[i] = biased_int(st[c * 128u + r], fk[c]);
+          for (unsigned i = 0u; i < 16u; ++i) {
+            const unsigned c = 16u * kg + i;
+            w[i] = biased_int(st[c * 128u + ct], fk[c]);
+          }
+          uint4 pl[kDig];
+          digits16(w, pl);
+          uint8_t *const dst = sm + kOffUA + (ct >> 3) * 512u + kg * 128u + (ct & 7u) * 16u;
+#pragma unroll
+          for (unsigned t = 0u; t < kDig; ++t)
+            *reinterpret_cast<uint4 *>(dst + t * kUAPlane) = pl[t];
         }
-        uint4 pl[kDig];
-        digits16(w, pl);
-        uint8_t *const dst = sm + kOffUA + (r >> 3) * 512u + kg * 128u + (r & 7u) * 16u;
+      }
+      fence_async_shared();
+      bar_sync(1u, 128u);
+      if (ct < 64u && k + 1u < it1)
+        next_cmax = col_word(item_of(P, k + 1u));
+      if (lead) {
+        if (k + 2u < it1) // the tile is cut: its buffer takes the item two ahead
+          load_tile(P, item_of(P, k + 2u), sm + kOffUStage + buf * kUStage, &bar[kBarFull + buf]);
+        const uint64_t a0 = sdesc(sbase + kOffUA, 128u, 512u), b0 = sdesc(sbase + kOffUB, 128u, 512u);
 #pragma unroll
-        for (unsigned t = 0u; t < kDig; ++t)
-          *reinterpret_cast<uint4 *>(dst + t * kUAPlane) = pl[t];
+        for (unsigned h = 0u; h < 2u; ++h) {
+          // the half's TMEM is drained by the epilogue of the previous item
+          if (n > 0u && !wait_or_abort(&bar[kBarFree + h], (n - 1u) & 1u, abort_flag)) {
+            *abort_flag = 1;
+            break;
+          }
+          tc_fence_after();
+#pragma unroll
+          for (unsigned kh = 0u; kh < 2u; ++kh)
+#pragma unroll
+            for (unsigned t = 0u; t < kDig; ++t)
+              mma_i8(tmem + h * 224u + t * 32u, a0 + ((t * kUAPlane + kh * 256u) >> 4),
+                     b0 + ((h * kBHalf + kh * 256u) >> 4), idesc_i8(128u, 32u * (kDig - t)),
+                     (t == 0u && kh == 0u) ? 0u : 1u);
+          mma_commit(&bar[kBarMma + h]);
+        }
       }
     }
-    fence_async_shared();
-    __syncthreads();
-    long long c2 = rec ? clock64() : 0;
-    if (tid < 64u && k + 1u < it1)
-      next_cmax = col_word(item_of(P, k + 1u));
-    if (tid == 0u) {
-      if (k + 2u < it1) // the tile is cut: its buffer takes the item two ahead
-        load_tile(P, item_of(P, k + 2u), sm + kOffUStage + buf * kUStage, &bar[buf]);
-      tc_fence_after();
-      // A = digit plane t of the tile (K half kh), B = planes u0 .. u0 + n - 1
-      // of V_loc side by side: D block t + u0 + i gets group t + u0 + i
-      const uint64_t a0 = sdesc(sbase + kOffUA, 128u, 512u), b0 = sdesc(sbase + kOffUB, 128u, 512u);
-#pragma unroll
-      for (unsigned kh = 0u; kh < 2u; ++kh) {
-#define GJX_UMMA(T, U0, NN)                                                                                          \
-  mma_i8(tmem + ((T) + (U0)) * 64u, a0 + (((T) * kUAPlane + kh * 256u) >> 4),                                        \
-         b0 + (((U0) * kBPlane + kh * 256u) >> 4), idesc_i8(128u, (NN) * 64u), ((T) == 0u && kh == 0u) ? 0u : 1u)
-        GJX_UMMA(0u, 0u, 4u);
-        GJX_UMMA(0u, 4u, 3u);
-        GJX_UMMA(1u, 0u, 4u);
-        GJX_UMMA(1u, 4u, 2u);
-        GJX_UMMA(2u, 0u, 4u);
-        GJX_UMMA(2u, 4u, 1u);
-        GJX_UMMA(3u, 0u, 4u);
-        GJX_UMMA(4u, 0u, 3u);
-        GJX_UMMA(5u, 0u, 2u);
-        GJX_UMMA(6u, 0u, 1u);
-#undef GJX_UMMA
+  }
+  else {
+    // ------------------------------ epilogue -------------------------------
+    const unsigned q4 = warp, r = q4 * 32u + lane; // TMEM lanes of this warp: the tile's rows
+    for (unsigned k = it0, n = 0u; k < it1; ++k, ++n) {
+      const Item it = item_of(P, k);
+      const unsigned buf = n & 1u;
+      if (bar_or(2u, 128u, !wait_or_abort(&bar[kBarMeta + buf], (n >> 1) & 1u, abort_flag))) {
+        *abort_flag = 1;
+        break;
       }
-      mma_commit(&bar[3]);
-    }
-    if (__syncthreads_or(!mbar_wait_bounded(&bar[3], n & 1u, kWait))) {
-      failed = true;
-      break;
-    }
-    tc_fence_after();
-    long long c3 = rec ? clock64() : 0;
-    {
-      // warp w: TMEM lanes 32 (w % 4) .. (tile rows), output columns 32 (w / 4) ..
-      // in two chunks of 16 (each within one block of the pair)
-      const unsigned q4 = warp & 3u, half = warp >> 2, r = q4 * 32u + lane;
       double *const out = it.isV ? P.V : P.G;
       const size_t ld = it.isV ? P.ldV : P.ldG;
       const bool inside = it.row0 + r < it.rows;
+      bool ok = true;
 #pragma unroll 1
-      for (unsigned ch = 0u; ch < 2u; ++ch) {
-        const unsigned j0 = half * 32u + ch * 16u;
-        int acc[kDig][16];
-#pragma unroll
-        for (unsigned g = 0u; g < kDig; ++g)
-          tmem_ld16(tmem + ((q4 * 32u) << 16) + g * 64u + j0, acc[g]);
-        double f[16];
-#pragma unroll
-        for (unsigned kk = 0u; kk < 16u; ++kk)
-          f[kk] = fo[j0 + kk];
-        double *const col0 = out + ((half ? it.jBlk : it.iBlk) * kBW + ch * 16u) * ld + it.row0 + r;
-        tmem_wait_ld();
-#pragma unroll
-        for (unsigned kk = 0u; kk < 16u; ++kk) {
-          const double c = recombine_u(acc[0][kk], acc[1][kk], acc[2][kk], acc[3][kk], acc[4][kk], acc[5][kk],
-                                       acc[6][kk]) * f[kk];
-          if (inside)
-            col0[kk * ld] = c;
-          const uint32_t m = __reduce_max_sync(0xffffffffu, abs_hi(c)); // rows beyond the matrix hold 0
-          if (lane == 0u)
-            cm[q4 * 64u + j0 + kk] = m;
+      for (unsigned h = 0u; h < 2u && ok; ++h) {
+        if (bar_or(2u, 128u, !wait_or_abort(&bar[kBarMma + h], n & 1u, abort_flag))) {
+          *abort_flag = 1;
+          ok = false;
+          break;
         }
+        tc_fence_after();
+        double *const colh = out + (size_t)((h ? it.jBlk : it.iBlk) * kBW) * ld + it.row0 + r;
+#pragma unroll 1
+        for (unsigned ch = 0u; ch < 2u; ++ch) {
+          const unsigned j0 = h * 32u + ch * 16u;
+          int acc[kDig][16];
+#pragma unroll
+          for (unsigned g = 0u; g < kDig; ++g)
+            tmem_ld16(tmem + ((q4 * 32u) << 16) + h * 224u + g * 32u + ch * 16u, acc[g]);
+          double f[16];
+#pragma unroll
+          for (unsigned kk = 0u; kk < 16u; ++kk)
+            f[kk] = fo[buf * 64u + j0 + kk];
+          tmem_wait_ld();
+#pragma unroll
+          for (unsigned kk = 0u; kk < 16u; ++kk) {
+            const double c = recombine_u(acc[0][kk], acc[1][kk], acc[2][kk], acc[3][kk], acc[4][kk], acc[5][kk],
+                                         acc[6][kk]) * f[kk];
+            if (inside)
+              colh[(size_t)(ch * 16u + kk) * ld] = c;
+            const uint32_t m = __reduce_max_sync(0xffffffffu, abs_hi(c)); // rows beyond the matrix hold 0
+            if (lane == 0u)
+              cm[q4 * 64u + j0 + kk] = m;
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0u)
+          mbar_arrive(&bar[kBarFree + h]);
       }
-    }
-    tc_fence_before();
-    __syncthreads();
-    if (rec) {
-      const long long c4 = clock64();
-      P.clk[5] += c1 - c0;
-      P.clk[6] += c2 - c1;
-      P.clk[7] += c3 - c2;
-      P.clk[8] += c4 - c3;
-      P.clk[9] += 1;
-    }
-    if (tid < 64u) {
-      const uint32_t m = max(max(cm[tid], cm[64u + tid]), max(cm[128u + tid], cm[192u + tid]));
-      const unsigned gc = (tid < kBW) ? it.iBlk * kBW + tid : it.jBlk * kBW + tid - kBW;
-      if (m)
-        atomicMax(&cmax[(P.parity ^ 1u) * P.ncol + gc], m);
+      if (!ok)
+        break;
+      bar_sync(2u, 128u); // the item's row-quarter maxima are written
+      if (r < 64u) {
+        const uint32_t m = max(max(cm[r], cm[64u + r]), max(cm[128u + r], cm[192u + r]));
+        const unsigned gc = (r < kBW) ? it.iBlk * kBW + r : it.jBlk * kBW + r - kBW;
+        if (m)
+          atomicMax(&(it.isV ? P.cmaxV : P.cmaxG)[(P.parity ^ 1u) * P.ncol + gc], m);
+      }
+      bar_sync(2u, 128u);
     }
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 0u)
     tmem_dealloc(tmem);
-  if (failed && tid == 0u)
+  if (*abort_flag && tid == 0u)
     set_err(P);
 }
 
