@@ -733,10 +733,15 @@ def main():
     ap.add_argument("--accuracy", action="store_true", help="add pp80 figures of the last decomposition")
     ap.add_argument("--shard", action="store_true", help="c5 over N ranks: split one batch instead of N batches")
     ap.add_argument("--count", type=int, default=0, help="c5: matrices in the batch (default 4096; profiling runs)")
+    ap.add_argument("--alg", type=int, default=-1, help="override the workload's ALG (studies; the config says so)")
     ap.add_argument("--form", default="plain", choices=["plain", "split"],
                     help="plain FP64 (the drop-in) or the split-precision form (gjx_hypJacL2_split)")
     args = ap.parse_args()
     _use(args.config)
+    if args.alg >= 0 and args.alg != ALG:
+        WORKLOADS[args.config] = dict(WORKLOADS[args.config], alg=args.alg,
+                                      workload=WORKLOADS[args.config]["workload"] + f"; ALG {args.alg} instead")
+        _use(args.config)
     if args.impl == "reference":
         return reference_arm(args)
     if args.config == "c5":
