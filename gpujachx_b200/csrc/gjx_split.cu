@@ -261,10 +261,11 @@ __device__ __forceinline__ uint32_t abs_hi(const double x)
 // ---------------------------------------------------------------------------
 // sp_pair_kernel
 // ---------------------------------------------------------------------------
-// Gram staging: 3 stages of one 64-row tile of the pair's 64 columns, four
+// Gram staging: kGStages stages of one 64-row tile of the pair's 64 columns, four
 // boxes {66 rows, 1 tile, 16 columns}: column c at c * 66 doubles (528 bytes,
 // an odd number of 16-byte granules: 8 consecutive columns in 8 bank groups)
 constexpr unsigned kGStages = 3u;
+constexpr unsigned kBarPlanes = kGStages; // [2] mbarriers after the stages': a plane buffer's MMAs done
 constexpr uint32_t kGBox = 66u * 16u * 8u;         // 8448 bytes
 constexpr uint32_t kGStageBytes = 4u * kGBox;       // 33792
 // digit planes of a 64-row tile: 2 chunks of 32 rows x 8 plane slots x 2 KB
@@ -291,6 +292,7 @@ constexpr uint32_t kOffScale = kOffS0 + 4096u;                               // 
 constexpr uint32_t kOffRed = kOffScale + 512u;                               // 64 unsigned
 constexpr uint32_t kOffBar = kOffRed + 256u;                                 // 8 mbarriers
 constexpr uint32_t kOffTmem = kOffBar + 64u;
+static_assert(kGStages + 2u <= 8u, "stage and plane-buffer mbarriers must fit their region");
 constexpr uint32_t kPairSmem = kOffTmem + 16u;
 static_assert(kPairSmem <= 227u * 1024u, "shared memory of sp_pair_kernel");
 
@@ -500,7 +502,7 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
   const unsigned pair = blockIdx.x;
   const uint16_t *const blk = P.strat1 + ((size_t)P.step * P.pairs + pair) * 2u;
   const unsigned iBlk = blk[0], jBlk = blk[1];
-  uint64_t *const bar = reinterpret_cast<uint64_t *>(sm + kOffBar); // [0..2] stage full, [3..4] planes free
+  uint64_t *const bar = reinterpret_cast<uint64_t *>(sm + kOffBar); // stages full, then planes free
   uint32_t *const tmem_holder = reinterpret_cast<uint32_t *>(sm + kOffTmem);
   int *const eG = reinterpret_cast<int *>(sm + kOffScale);
   int *const eV = eG + 64;
@@ -515,7 +517,7 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
     t_start = clock64();
   if (tid == 0u) {
     s_fail = 0;
-    for (unsigned i = 0u; i < 5u; ++i)
+    for (unsigned i = 0u; i < kGStages + 2u; ++i)
       mbar_init(&bar[i], 1u);
     mbar_fence_init();
   }
@@ -548,14 +550,16 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
   // slicing task of this thread: column x, rows 16 rg .. 16 rg + 15 of the tile
   const unsigned x = tid & 63u, rg = tid >> 6;
   const double fx = cut_factor(eG[x]);
+  unsigned i_stop = ntiles; // the tiles taken in (all, unless a wait gave up)
   for (unsigned i = 0u; i < ntiles; ++i) {
     const unsigned s = i % kGStages, b = i & 1u;
     int bad = !mbar_wait_bounded(&bar[s], (i / kGStages) & 1u, kWait);
-    if (i >= 2u && !mbar_wait_bounded(&bar[3u + b], ((i - 2u) >> 1) & 1u, kWait))
+    if (i >= 2u && !mbar_wait_bounded(&bar[kBarPlanes + b], ((i - 2u) >> 1) & 1u, kWait))
       bad = 1;
     if (__syncthreads_or(bad)) { // every thread leaves the loop together
       if (tid == 0u)
         s_fail = 1;
+      i_stop = i;
       break;
     }
     {
@@ -611,7 +615,7 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
         GJX_GMMA(3u, 0u, 1u, 1u);
 #undef GJX_GMMA
       }
-      mma_commit(&bar[3u + b]);
+      mma_commit(&bar[kBarPlanes + b]);
     }
   }
   // the last commit covers every MMA
@@ -619,7 +623,7 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
   int bad = s_fail;
   if (!bad && ntiles) {
     const unsigned last = ntiles - 1u;
-    bad = !mbar_wait_bounded(&bar[3u + (last & 1u)], (last >> 1) & 1u, kWait);
+    bad = !mbar_wait_bounded(&bar[kBarPlanes + (last & 1u)], (last >> 1) & 1u, kWait);
   }
   const bool failed = __syncthreads_or(bad) != 0;
   tc_fence_after();
@@ -670,6 +674,15 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
         R[y * kLd + xr] = scale2(recombine(sg[0], sg[1], sg[2], sg[3], sg[4], sg[5], sg[6]), eG[xr] + eG[y] - 36);
       }
     }
+  }
+  if (failed && tid == 0u) {
+    // before the shared memory and TMEM are given up: the copies still in
+    // flight (tiles i_stop .. i_stop + kGStages - 1, as issued) and the MMAs
+    // of the last tile taken complete (bounded)
+    for (unsigned t = i_stop; t < ntiles && t < i_stop + kGStages; ++t)
+      (void)mbar_wait_bounded(&bar[t % kGStages], (t / kGStages) & 1u, kWait / 8);
+    if (i_stop > 0u)
+      (void)mbar_wait_bounded(&bar[kBarPlanes + ((i_stop - 1u) & 1u)], ((i_stop - 1u) >> 1) & 1u, kWait / 8);
   }
   tc_fence_before();
   __syncthreads();
@@ -943,9 +956,14 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
     // ------------------------------- cutters -------------------------------
     const unsigned ct = tid - 128u; // 0..127: row ct of the tile
     const bool lead = ct == 0u;
+    // the lead's count of the asynchronous work it started and saw finish, for
+    // the drain on the failure path: tile loads per buffer, B loads, commits per half
+    unsigned l_iss[2] = {0u, 0u}, l_done[2] = {0u, 0u}, b_iss = 0u, b_done = 0u, m_iss[2] = {0u, 0u};
     if (lead)
-      for (unsigned k = it0; k < it1 && k < it0 + 2u; ++k)
+      for (unsigned k = it0; k < it1 && k < it0 + 2u; ++k) {
         load_tile(P, item_of(P, k), sm + kOffUStage + (k - it0) * kUStage, &bar[kBarFull + (k - it0)]);
+        ++l_iss[k - it0];
+      }
     auto col_word = [&](const Item &x) -> uint32_t {
       const unsigned gc = (ct < kBW) ? x.iBlk * kBW + ct : x.jBlk * kBW + ct - kBW;
       return (x.isV ? P.cmaxV : P.cmaxG)[P.parity * P.ncol + gc];
@@ -964,13 +982,18 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
         mbar_arrive_expect_tx(&bar[kBarB], kBopBytes);
         bulk_g2s(sm + kOffUB, P.bop + ((size_t)it.pair * (ACCV ? 2u : 1u) + (it.isV ? 1u : 0u)) * kBopBytes,
                  kBopBytes, &bar[kBarB]);
+        ++b_iss;
       }
       if (ct < 64u)
         fk[ct] = cut_factor(col_exp(next_cmax));
-      if (ok && newb)
+      if (ok && newb) {
         ok = wait_or_abort(&bar[kBarB], nb & 1u, abort_flag);
-      if (ok)
+        b_done += ok ? 1u : 0u;
+      }
+      if (ok) {
         ok = wait_or_abort(&bar[kBarFull + buf], (n >> 1) & 1u, abort_flag);
+        l_done[buf] += ok ? 1u : 0u;
+      }
       if (newb) {
         key = it.key;
         ++nb;
@@ -1008,8 +1031,10 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
       if (ct < 64u && k + 1u < it1)
         next_cmax = col_word(item_of(P, k + 1u));
       if (lead) {
-        if (k + 2u < it1) // the tile is cut: its buffer takes the item two ahead
+        if (k + 2u < it1) { // the tile is cut: its buffer takes the item two ahead
           load_tile(P, item_of(P, k + 2u), sm + kOffUStage + buf * kUStage, &bar[kBarFull + buf]);
+          ++l_iss[buf];
+        }
         const uint64_t a0 = sdesc(sbase + kOffUA, 128u, 512u), b0 = sdesc(sbase + kOffUB, 128u, 512u);
 #pragma unroll
         for (unsigned h = 0u; h < 2u; ++h) {
@@ -1027,8 +1052,22 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
                      b0 + ((h * kBHalf + kh * 256u) >> 4), idesc_i8(128u, 32u * (kDig - t)),
                      (t == 0u && kh == 0u) ? 0u : 1u);
           mma_commit(&bar[kBarMma + h]);
+          ++m_iss[h];
         }
       }
+    }
+    if (lead && *abort_flag) {
+      // before the shared memory and TMEM are given up, what was started
+      // completes (bounded): the tile loads and the B load not yet waited
+      // for, and each half's last MMAs
+      for (unsigned b = 0u; b < 2u; ++b)
+        if (l_iss[b] > l_done[b])
+          (void)mbar_wait_bounded(&bar[kBarFull + b], (l_iss[b] - 1u) & 1u, kWait / 8);
+      if (b_iss > b_done)
+        (void)mbar_wait_bounded(&bar[kBarB], (b_iss - 1u) & 1u, kWait / 8);
+      for (unsigned h = 0u; h < 2u; ++h)
+        if (m_iss[h] > 0u)
+          (void)mbar_wait_bounded(&bar[kBarMma + h], (m_iss[h] - 1u) & 1u, kWait / 8);
     }
   }
   else {
