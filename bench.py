@@ -524,8 +524,9 @@ def main_batch(args):
     hbm, peak_kind = _peaks()
     roof = {"bound": "hbm", "achieved": nbytes / t_s / 1e9, "peak": hbm, "unit": "GB/s",
             "frac": nbytes / t_s / 1e9 / hbm, "traffic": None,
-            "kernel": ("gjx::l1_batch_flow_kernel<true,true,%d>" if tuned["mode"] else "gjx::l1_batch_kernel<true,true,%d>")
-            % width,
+            "kernel": ("gjx::l1_batchn_kernel<true,true>" if width == 3 else
+                       ("gjx::l1_batch_flow_kernel<true,true,%d>" if tuned["mode"] else
+                        "gjx::l1_batch_kernel<true,true,%d>") % width),
             "peak_kind": f"{peak_kind} HBM copy bandwidth",
             "note": "algorithmic bytes of all sweeps run, over the device time of the whole batched call",
             "fp64_tflops": flops / t_s / 1e12, "launches_per_step": prof["launches"] // max(1, args.steps)}

@@ -50,7 +50,8 @@ Strat g_strat;
 int g_verbose = 1;
 int g_sweep_mode = -1; // -1 automatic (the tuned choice, else per step), 0 per outer step, 1 one launch per sweep
 unsigned g_split = 0u;  // CTAs per block pair: 0 automatic (the tuned choice, else by the SM count), else 1, 2, 4
-unsigned g_pairs_per_cta = 0u; // block pairs a CTA takes at a time: 0 automatic, 1, or 2
+unsigned g_pairs_per_cta = 0u; // block pairs a CTA takes at a time: 0 automatic, 1, 2, or 3 (batched form:
+                               // one per CTA of 4 warps, two CTAs per SM)
 unsigned g_variant = 0u; // pivot-block factor: 0 Gram + Cholesky, 1 QR (-DUSE_QR), 2 QR + Drmac (-DUSE_DRMAC)
 int g_batch_mode = -1;   // batched form: -1 the tuned choice (else per step), 0 one launch per step, 1 per sweep
 unsigned g_batch_cap = 0u; // nonzero: the batched form stops after this many sweeps (the autotuner's runs)
@@ -587,7 +588,7 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
   int dev = 0, sms = 148;
   GJX_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
   GJX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-  unsigned width = (g_pairs_per_cta == 1u) ? 1u : 2u;
+  unsigned width = (g_pairs_per_cta == 1u) ? 1u : (g_pairs_per_cta == gjx::kWidthHalf) ? gjx::kWidthHalf : 2u;
   int mode = g_batch_mode;
   {
     const auto t = g_batch_tuned.find(batch_key(nmat, nrow, ncol, nplus));
@@ -598,6 +599,8 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
         mode = t->second.second;
     }
   }
+  if (width == gjx::kWidthHalf)
+    mode = 0; // the CTAs of 4 warps run the per-step launches
   const unsigned cap = g_batch_cap ? g_batch_cap : gjx::kNSweep;
   if (mode == 1) { // one launch per sweep (the dataflow form)
     std::vector<uint32_t> fitems;
@@ -692,7 +695,8 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
   cudaError_t ce = cudaSuccess;
   const gjx::BatchStep bs{d_mats, d_items, (unsigned)items.size(), d_ks, d_q, d_done, d_err};
   const gjx::BatchSweep sw{d_mats, d_ks, d_cvg, d_done, d_swp, d_gs, d_gb, d_q, d_act, nmat};
-  const unsigned ctas = std::min<unsigned>((unsigned)sms, (unsigned)items.size());
+  const unsigned ctas =
+      std::min<unsigned>((width == gjx::kWidthHalf ? 2u : 1u) * (unsigned)sms, (unsigned)items.size());
   for (unsigned k = 0u; k < kLaunches && ce == cudaSuccess; ++k) {
     ce = gjx::launch_batch_step(cdsort, full, width, bs, ctas, st);
     if (ce == cudaSuccess)
@@ -1292,7 +1296,7 @@ void gjx_set_variant(const unsigned v)
 void gjx_set_pairs_per_cta(const unsigned w)
 {
   std::lock_guard<std::mutex> lk(g_mtx);
-  g_pairs_per_cta = (w == 1u || w == 2u) ? w : 0u;
+  g_pairs_per_cta = (w == 1u || w == 2u || w == gjx::kWidthHalf) ? w : 0u;
 }
 
 int gjx_autotune_batched(const unsigned routine, const unsigned nmat, const unsigned *const nrow,
@@ -1356,8 +1360,10 @@ int gjx_autotune_batched(const unsigned routine, const unsigned nmat, const unsi
   float best = 3.0e38f;
   std::pair<unsigned, int> pick{2u, 0};
   int rc = 0;
-  for (unsigned width : {2u, 1u}) {
+  for (unsigned width : {2u, 1u, gjx::kWidthHalf}) {
     for (int mode : {0, 1}) {
+      if (width == gjx::kWidthHalf && mode == 1)
+        continue; // per-step launches only
       g_pairs_per_cta = width;
       g_batch_mode = mode;
       float ms = 0.0f;

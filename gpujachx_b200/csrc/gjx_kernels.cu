@@ -1409,6 +1409,215 @@ __global__ void __launch_bounds__(kThreads, 1) l1_batch_kernel(const __grid_cons
   }
 }
 
+// ---------------------------------------------------------------------------
+// One block pair on a CTA of 4 warps (batched form, two such CTAs per SM).
+// The arithmetic is that of pair_step with one CTA per pair -- the Gram
+// chains of gram_tile2 on warps 0-2 (warp 3 issues the tile copies), the
+// Cholesky factorisation and quarter-warp inner sweeps of pair_step2's warp
+// groups, pair_step's update tiles (warp w takes row groups w and w + 4 of
+// every stage) -- so every matrix gets the bits of its single call.  Shared
+// memory (86 KB): the Gram's 4 stages of one 64-row tile, later one update
+// buffer; R, V_loc.  With one buffer a stage's copy waits for the store of
+// the stage before; the other CTA of the SM runs meanwhile, and its serial
+// phases (Cholesky, inner sweeps: chains of divides and square roots that
+// leave the pipes idle) overlap this CTA's Gram and update, and the reverse.
+// ---------------------------------------------------------------------------
+constexpr unsigned kNThreads = 128u;
+constexpr unsigned kNGStages = 4u;
+constexpr unsigned kNIssuer = 96u; // lane 0 of warp 3
+constexpr unsigned kNRegion = (kNGStages * kGramTileLd > kUpdStage) ? kNGStages * kGramTileLd : kUpdStage;
+constexpr unsigned kNOffR = kNRegion; // R, 32x32 (later B^T, 32x34)
+constexpr unsigned kNOffVl = kNOffR + 32u * kVTLd;
+constexpr unsigned kNOffS0 = kNOffVl + 1024u;
+constexpr unsigned kNOffRed = kNOffS0 + 128u;
+constexpr unsigned kNOffBar = kNOffRed + 16u; // [0..3] Gram stages, [4] the update buffer
+constexpr unsigned kNSmemDoubles = kNOffBar + 8u;
+static_assert(2u * (kNSmemDoubles * sizeof(double) + 1024u) <= 228u * 1024u, "two CTAs per SM");
+size_t batchn_smem_bytes() { return (size_t)kNSmemDoubles * sizeof(double); }
+
+template <bool SORT, bool ACCV>
+__device__ __forceinline__ void pair_step_n(const StepParams &P, const unsigned step, const unsigned pair,
+                                            double *const sm)
+{
+  double *const stg = sm;
+  double *const R = sm + kNOffR;
+  double *const Vl = sm + kNOffVl;
+  uint8_t *const s0 = reinterpret_cast<uint8_t *>(sm + kNOffS0);
+  unsigned *const red = reinterpret_cast<unsigned *>(sm + kNOffRed);
+  uint64_t *const bars = reinterpret_cast<uint64_t *>(sm + kNOffBar);
+  const unsigned tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+  const size_t pidx = ((size_t)step * P.pairs + pair) * 2u;
+  const unsigned iBlk = P.strat1[pidx + 0u], jBlk = P.strat1[pidx + 1u];
+
+  for (unsigned i = tid; i < 256u; i += kNThreads)
+    reinterpret_cast<uint32_t *>(s0)[i] = reinterpret_cast<const uint32_t *>(P.strat0)[i];
+  if (tid == 0u) {
+    for (unsigned b = 0u; b < 5u; ++b)
+      mbar_init(&bars[b], 1u);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  // ------------------------------ 1. Gram --------------------------------
+  const unsigned ntile = P.nrow >> 6;
+  unsigned gx0 = 0u, gy = 0u, gy1 = 0u;
+  const bool gthr = gram_lane2(warp, lane, gx0, gy, gy1);
+  double gacc[4][2] = {{+0.0, +0.0}, {+0.0, +0.0}, {+0.0, +0.0}, {+0.0, +0.0}};
+  auto issue_gram = [&](const unsigned k) { // tile k into stage k mod 4
+    const unsigned s = k % kNGStages;
+    double *const st = stg + s * kGramTileLd;
+    mbar_arrive_expect_tx(&bars[s], 2u * kGramBoxBytes);
+    tma_load_3d(st, &P.tmGram, 0, (int)k, (int)(iBlk * kNColB), &bars[s]);
+    tma_load_3d(st + 16u * kGramColLd, &P.tmGram, 0, (int)k, (int)(jBlk * kNColB), &bars[s]);
+  };
+  if (tid == kNIssuer)
+    for (unsigned k = 0u; k + 1u < kNGStages && k < ntile; ++k)
+      issue_gram(k);
+  unsigned k = 0u;
+  int failed = 0;
+  for (; k < ntile; ++k) {
+    if (tid == kNIssuer && k + kNGStages - 1u < ntile)
+      issue_gram(k + kNGStages - 1u); // into the stage released after tile k - 1
+    int fail = 0;
+    if (warp < 3u) {
+      if (!mbar_wait_bounded(&bars[k % kNGStages], (k / kNGStages) & 1u, kWaitLimit))
+        fail = 1;
+      else if (gthr)
+        gram_tile2(stg + (k % kNGStages) * kGramTileLd, 0u, gx0, gy, gy1, gacc);
+    }
+    failed = __syncthreads_or(fail);
+    if (failed)
+      break;
+  }
+  if (failed) {
+    if (tid == 0u) { // the copies in flight land (bounded) before anything else, report
+      for (unsigned q = k; q < ntile && q < k + kNGStages; ++q)
+        (void)mbar_wait_bounded(&bars[q % kNGStages], (q / kNGStages) & 1u, kWaitLimit / 8);
+      atomicOr(P.err, kErrWaitTimeout);
+    }
+    return;
+  }
+  if (gthr) {
+#pragma unroll
+    for (unsigned u = 0u; u < 4u; ++u)
+#pragma unroll
+      for (unsigned v = 0u; v < 2u; ++v) {
+        const unsigned y = v ? gy1 : gy;
+        if (gx0 + u >= y)
+          R[y * 32u + gx0 + u] = gacc[u][v];
+      }
+  }
+  __syncthreads();
+
+  // the first update stage: its rows do not change before the update, so the
+  // copy overlaps the Cholesky and the inner sweeps
+  const unsigned nG = (P.nrow + kUpdRows - 1u) / kUpdRows;
+  const unsigned nst = nG + (ACCV ? (P.ncol + kUpdRows - 1u) / kUpdRows : 0u);
+  auto issue_upd = [&](const unsigned i) {
+    const bool isG = i < nG;
+    const CUtensorMap *const tm = isG ? &P.tmG : &P.tmV;
+    const int piece = (int)(((isG ? i : (i - nG)) * kUpdRows) >> 5);
+    mbar_arrive_expect_tx(&bars[4], 2u * kUpdBoxBytes);
+    tma_load_3d(stg, tm, 0, piece, (int)(iBlk * kNColB), &bars[4]);
+    tma_load_3d(stg + 16u * kUpdColLd, tm, 0, piece, (int)(jBlk * kNColB), &bars[4]);
+  };
+  if (tid == 0u && nst > 0u)
+    issue_upd(0u);
+
+  // ------------------- 2.-3. Cholesky and inner sweeps --------------------
+  for (unsigned i = tid; i < 1024u; i += kNThreads)
+    Vl[i] = ((i >> 5) == (i & 31u)) ? 1.0 : 0.0;
+  chol32_grp<4u>(R, tid, 0u);
+  __syncthreads();
+  int definite;
+  unsigned npos;
+  block_signature(P, iBlk, jBlk, definite, npos);
+  unsigned blk_s, blk_b;
+  inner_sweeps_q<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, lane, warp, 0u, blk_s, blk_b);
+  if (tid == 0u)
+    add_counts(P, blk_s, blk_b);
+  if (!SORT && !blk_s) { // no rotation: the block pair is unchanged
+    if (tid == 0u && nst > 0u && !mbar_wait_bounded(&bars[4], 0u, kWaitLimit))
+      atomicOr(P.err, kErrWaitTimeout); // the prefetched copy has landed before we leave
+    return;
+  }
+
+  // ------------------------------ 4. update -------------------------------
+  for (unsigned i = tid; i < 1024u; i += kNThreads) { // R is dead: B^T[s][c] = V_loc[s][c]
+    const unsigned c = i >> 5, s_ = i & 31u;
+    R[s_ * kVTLd + c] = E32(Vl, s_, c);
+  }
+  __syncthreads();
+  const unsigned sub = lane & 7u, cg8 = lane >> 3;
+  for (unsigned i = 0u; i < nst; ++i) {
+    if (tid == 0u && i > 0u) {
+      bulk_wait_read(); // the store of stage i - 1 has read the buffer out
+      issue_upd(i);
+    }
+    const int fail = !__all_sync(0xffffffffu, mbar_wait_bounded(&bars[4], i & 1u, kWaitLimit));
+    if (!fail) {
+#pragma unroll 1
+      for (unsigned h = 0u; h < 2u; ++h) { // row groups warp and warp + 4
+        double acc[4][8];
+        update_stage(stg, R, warp + 4u * h, sub, cg8, acc);
+        __syncwarp();
+        update_put(stg, acc, warp + 4u * h, sub, cg8);
+      }
+      fence_async_shared();
+    }
+    if (__syncthreads_or(fail)) {
+      if (tid == 0u) {
+        (void)mbar_wait_bounded(&bars[4], i & 1u, kWaitLimit / 8);
+        bulk_wait_all();
+        atomicOr(P.err, kErrWaitTimeout);
+      }
+      return;
+    }
+    if (tid == 0u) {
+      const bool isG = i < nG;
+      const CUtensorMap *const tm = isG ? &P.tmG : &P.tmV;
+      const int piece = (int)(((isG ? i : (i - nG)) * kUpdRows) >> 5);
+      tma_store_3d(tm, stg, 0, piece, (int)(iBlk * kNColB));
+      tma_store_3d(tm, stg + 16u * kUpdColLd, 0, piece, (int)(jBlk * kNColB));
+      bulk_commit();
+    }
+  }
+  if (tid == 0u)
+    bulk_wait_all(); // the stores are complete before the block pair counts as done
+}
+
+// The batched step on CTAs of 4 warps, two per SM: a CTA takes one block pair
+// at a time from the queue (the same queue, items and skips as
+// l1_batch_kernel).  The mbarriers are invalidated after each item.
+template <bool SORT, bool ACCV>
+__global__ void __launch_bounds__(kNThreads, 2) l1_batchn_kernel(const __grid_constant__ BatchStep B)
+{
+  extern __shared__ __align__(128) double sm[];
+  __shared__ unsigned item;
+  uint64_t *const bars = reinterpret_cast<uint64_t *>(sm + kNOffBar);
+  for (;;) {
+    if (threadIdx.x == 0u)
+      item = atomicAdd(B.queue, 1u);
+    __syncthreads();
+    const unsigned it = item;
+    const bool stop = (it >= B.nitems) || (*(volatile int *)B.err != 0);
+    __syncthreads(); // every thread has read item
+    if (stop)
+      break;
+    const uint32_t e = B.items[it];
+    const unsigned b = e >> 16u;
+    if (B.done[b])
+      continue;
+    const BatchMat &m = B.mats[b];
+    pair_step_n<SORT, ACCV>(m.p, B.kstep[b] % m.steps1, e & 0xffffu, sm);
+    __syncthreads();
+    if (threadIdx.x == 0u)
+      for (unsigned k = 0u; k < 5u; ++k)
+        mbar_inval(&bars[k]);
+    __syncthreads();
+  }
+}
+
 // One launch per sweep of the whole batch (the dataflow form): the CTAs take
 // (matrix, step, pair) items in queue order -- step-major, every matrix's
 // step s before any step s + 1 -- and an item waits until both of its blocks
@@ -1804,6 +2013,9 @@ template <bool S, bool A> static cudaError_t set_smem_batch()
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(l1_batch_kernel<S, A, 2u>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)batch2_smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(l1_batchn_kernel<S, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)batchn_smem_bytes());
   return e;
 }
 
@@ -1819,7 +2031,9 @@ cudaError_t batch_configure()
 template <bool S, bool A>
 static void batch_launch(const unsigned width, const BatchStep &b, const unsigned ctas, cudaStream_t s)
 {
-  if (width == 2u)
+  if (width == kWidthHalf)
+    l1_batchn_kernel<S, A><<<ctas, kNThreads, batchn_smem_bytes(), s>>>(b);
+  else if (width == 2u)
     l1_batch_kernel<S, A, 2u><<<ctas, kThreads, batch2_smem_bytes(), s>>>(b);
   else
     l1_batch_kernel<S, A, 1u><<<ctas, kThreads, l1_smem_bytes(), s>>>(b);

@@ -109,11 +109,13 @@ void gjx_set_split(unsigned n);
 
 /* Block pairs that a CTA takes at a time: 2 (the Cholesky factorisations
  * and inner sweeps of the two run concurrently on two groups of 4 warps), 1,
- * or 0 (default): automatic -- 2 in the batched form
- * (gjx_hypJacL2_batched), and in the per-step launches of a single matrix
- * with one CTA per block pair when a step has more block pairs than the GPU
- * has SMs (one wave of CTAs instead of two); else 1.  The results are the
- * same bits for every value. */
+ * 3 (batched form only: one block pair per CTA of 4 warps, two such CTAs per
+ * SM, so that one CTA's serial phases overlap the other's Gram and update;
+ * per-step launches), or 0 (default): automatic -- the batched autotuner's
+ * choice, else 2 in the batched form (gjx_hypJacL2_batched), and in the
+ * per-step launches of a single matrix with one CTA per block pair when a
+ * step has more block pairs than the GPU has SMs (one wave of CTAs instead of
+ * two); else 1.  The results are the same bits for every value. */
 void gjx_set_pairs_per_cta(unsigned w);
 
 /* The pivot-block factor of the reference's alternative builds, for
@@ -148,7 +150,7 @@ void gjx_autotune_clear(void);
  * previous step.  The results are the same bits either way. */
 void gjx_set_batch_mode(int mode);
 
-/* Autotuner of the batched form: times block pairs per CTA (2, 1) x launch
+/* Autotuner of the batched form: times block pairs per CTA (2, 1, 3) x launch
  * mode (per step, per sweep) on seeded random matrices of the batch's shapes
  * (nrow[b] x ncol[b], the signature kind of nplus[b]), `sweeps` sweeps each
  * (0: 1), and uses the fastest in later gjx_hypJacL2_batched calls on a
