@@ -599,8 +599,6 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
         mode = t->second.second;
     }
   }
-  if (width == gjx::kWidthHalf)
-    mode = 0; // the CTAs of 4 warps run the per-step launches
   const unsigned cap = g_batch_cap ? g_batch_cap : gjx::kNSweep;
   if (mode == 1) { // one launch per sweep (the dataflow form)
     std::vector<uint32_t> fitems;
@@ -639,7 +637,8 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
     cudaError_t ce = cudaSuccess;
     const gjx::BatchFlow bf{d_mats, d_fitems, d_fsteps, (unsigned)fitems.size(), d_q, d_done, d_ver, d_vofs, d_err};
     const gjx::BatchSweep sw{d_mats, d_ks, d_cvg, d_done, d_swp, d_gs, d_gb, d_q, d_act, nmat};
-    const unsigned ctas = std::min<unsigned>((unsigned)sms, (unsigned)fitems.size());
+    const unsigned ctas =
+        std::min<unsigned>((width == gjx::kWidthHalf ? 2u : 1u) * (unsigned)sms, (unsigned)fitems.size());
     for (unsigned k = 0u; k < kSweeps && ce == cudaSuccess; ++k) {
       ce = gjx::launch_batch_flow(cdsort, full, width, bf, ctas, st);
       if (ce == cudaSuccess)
@@ -1362,8 +1361,6 @@ int gjx_autotune_batched(const unsigned routine, const unsigned nmat, const unsi
   int rc = 0;
   for (unsigned width : {2u, 1u, gjx::kWidthHalf}) {
     for (int mode : {0, 1}) {
-      if (width == gjx::kWidthHalf && mode == 1)
-        continue; // per-step launches only
       g_pairs_per_cta = width;
       g_batch_mode = mode;
       float ms = 0.0f;

@@ -96,7 +96,7 @@ cudaError_t launch_wait_selftest(long long limit, int *timed_out, long long *cyc
 bool sweep_kernel_fits(bool sort, bool accv, const StepParams &p);
 cudaError_t launch_l1_sweep(bool sort, bool accv, const StepParams &p, cudaStream_t s);
 // width 1: one block pair per CTA at a time; 2: two (pair_step2);
-// kWidthHalf: one per CTA of 4 warps, two CTAs per SM (per-step launches only)
+// kWidthHalf: one per CTA of 4 warps, two CTAs per SM
 constexpr unsigned kWidthHalf = 3u;
 cudaError_t launch_batch_step(bool sort, bool accv, unsigned width, const BatchStep &b, unsigned ctas,
                               cudaStream_t s);

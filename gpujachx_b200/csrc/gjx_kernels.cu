@@ -1732,6 +1732,66 @@ __global__ void __launch_bounds__(kThreads, 1) l1_batch_flow_kernel(const __grid
   }
 }
 
+// The dataflow form on CTAs of 4 warps, two per SM: one item at a time, the
+// same queue, readiness waits and write counts as l1_batch_flow_kernel.
+template <bool SORT, bool ACCV>
+__global__ void __launch_bounds__(kNThreads, 2) l1_batchn_flow_kernel(const __grid_constant__ BatchFlow B)
+{
+  extern __shared__ __align__(128) double sm[];
+  __shared__ unsigned item, ok;
+  uint64_t *const bars = reinterpret_cast<uint64_t *>(sm + kNOffBar);
+  const unsigned tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0u)
+      item = atomicAdd(B.queue, 1u);
+    __syncthreads();
+    const unsigned it = item;
+    const bool stop = (it >= B.nitems) || (*(volatile int *)B.err != 0);
+    __syncthreads();
+    if (stop)
+      break;
+    const uint32_t e = B.items[it];
+    const unsigned stp = B.isteps[it], b = e >> 16u, q = e & 0xffffu;
+    if (B.done[b])
+      continue;
+    const BatchMat &m = B.mats[b];
+    const size_t pidx = ((size_t)stp * m.p.pairs + q) * 2u;
+    unsigned *const v = B.ver + B.vofs[b];
+    const unsigned iB = m.p.strat1[pidx], jB = m.p.strat1[pidx + 1u];
+    if (tid == 0u) { // both blocks written by the matrix's previous step (bounded)
+      ok = 1u;
+      const long long t0 = clock64();
+      while (ld_acquire(v + iB) < stp || ld_acquire(v + jB) < stp) {
+        if (*(volatile int *)B.err) {
+          ok = 0u;
+          break;
+        }
+        if (clock64() - t0 > kWaitLimit) {
+          atomicOr(B.err, kErrWaitTimeout);
+          ok = 0u;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __syncthreads();
+    if (!ok)
+      break;
+    asm volatile("fence.proxy.async;" ::: "memory"); // the copies below read what other SMs wrote
+    pair_step_n<SORT, ACCV>(m.p, stp, q, sm);
+    __threadfence();
+    __syncthreads();
+    if (tid == 0u) {
+      __threadfence();
+      atomicAdd(v + iB, 1u);
+      atomicAdd(v + jB, 1u);
+      for (unsigned k = 0u; k < 5u; ++k)
+        mbar_inval(&bars[k]);
+    }
+    __syncthreads();
+  }
+}
+
 // after a sweep of the dataflow form: per matrix still sweeping, the sweep's
 // counter folded into its totals and the convergence test (no big rotation,
 // or the sweep cap); its block counts and the queue cleared for the next
@@ -2061,8 +2121,12 @@ template <bool S, bool A> static cudaError_t set_smem_flow()
                                        (int)l1_smem_bytes());
   if (e != cudaSuccess)
     return e;
-  return cudaFuncSetAttribute(l1_batch_flow_kernel<S, A, 2u>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)batch2_smem_bytes());
+  e = cudaFuncSetAttribute(l1_batch_flow_kernel<S, A, 2u>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)batch2_smem_bytes());
+  if (e != cudaSuccess)
+    return e;
+  return cudaFuncSetAttribute(l1_batchn_flow_kernel<S, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)batchn_smem_bytes());
 }
 
 cudaError_t flow_configure()
@@ -2077,7 +2141,9 @@ cudaError_t flow_configure()
 template <bool S, bool A>
 static void flow_launch(const unsigned width, const BatchFlow &b, const unsigned ctas, cudaStream_t s)
 {
-  if (width == 2u)
+  if (width == kWidthHalf)
+    l1_batchn_flow_kernel<S, A><<<ctas, kNThreads, batchn_smem_bytes(), s>>>(b);
+  else if (width == 2u)
     l1_batch_flow_kernel<S, A, 2u><<<ctas, kThreads, batch2_smem_bytes(), s>>>(b);
   else
     l1_batch_flow_kernel<S, A, 1u><<<ctas, kThreads, l1_smem_bytes(), s>>>(b);

@@ -110,8 +110,8 @@ void gjx_set_split(unsigned n);
 /* Block pairs that a CTA takes at a time: 2 (the Cholesky factorisations
  * and inner sweeps of the two run concurrently on two groups of 4 warps), 1,
  * 3 (batched form only: one block pair per CTA of 4 warps, two such CTAs per
- * SM, so that one CTA's serial phases overlap the other's Gram and update;
- * per-step launches), or 0 (default): automatic -- the batched autotuner's
+ * SM, so that one CTA's serial phases overlap the other's Gram and update),
+ * or 0 (default): automatic -- the batched autotuner's
  * choice, else 2 in the batched form (gjx_hypJacL2_batched), and in the
  * per-step launches of a single matrix with one CTA per block pair when a
  * step has more block pairs than the GPU has SMs (one wave of CTAs instead of
