@@ -524,7 +524,8 @@ def main_batch(args):
     hbm, peak_kind = _peaks()
     roof = {"bound": "hbm", "achieved": nbytes / t_s / 1e9, "peak": hbm, "unit": "GB/s",
             "frac": nbytes / t_s / 1e9 / hbm, "traffic": None,
-            "kernel": ("gjx::l1_batchn_kernel<true,true>" if width == 3 else
+            "kernel": ("gjx::l1_batchn2_kernel<true,true>" if width == 4 else
+                       "gjx::l1_batchn_kernel<true,true>" if width == 3 else
                        ("gjx::l1_batch_flow_kernel<true,true,%d>" if tuned["mode"] else
                         "gjx::l1_batch_kernel<true,true,%d>") % width),
             "peak_kind": f"{peak_kind} HBM copy bandwidth",

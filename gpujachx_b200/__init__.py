@@ -332,8 +332,8 @@ def autotune_batched(routine: int, nrows, ncols, nplus, sweeps: int = 1) -> dict
     """Time the batched form's configurations (block pairs per CTA, launch per
     step or per sweep) on seeded random matrices of these shapes and keep the
     fastest for later batches of the same shapes (gjx_autotune_batched);
-    returns {"pairs_per_cta": 1, 2 or 3 (one per CTA of 4 warps, two CTAs per
-    SM), "mode": 0 per step / 1 per sweep}."""
+    returns {"pairs_per_cta": 1, 2, 3 (one per CTA of 4 warps, two CTAs per
+    SM) or 4 (two per CTA of 4 warps), "mode": 0 per step / 1 per sweep}."""
     n = len(ncols)
     U = ctypes.c_uint * n
     out = (ctypes.c_uint * 2)()

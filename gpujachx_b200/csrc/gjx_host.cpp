@@ -588,7 +588,8 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
   int dev = 0, sms = 148;
   GJX_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
   GJX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-  unsigned width = (g_pairs_per_cta == 1u) ? 1u : (g_pairs_per_cta == gjx::kWidthHalf) ? gjx::kWidthHalf : 2u;
+  unsigned width = (g_pairs_per_cta == 1u || g_pairs_per_cta == gjx::kWidthHalf ||
+                    g_pairs_per_cta == gjx::kWidthHalf2) ? g_pairs_per_cta : 2u;
   int mode = g_batch_mode;
   {
     const auto t = g_batch_tuned.find(batch_key(nmat, nrow, ncol, nplus));
@@ -637,8 +638,9 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
     cudaError_t ce = cudaSuccess;
     const gjx::BatchFlow bf{d_mats, d_fitems, d_fsteps, (unsigned)fitems.size(), d_q, d_done, d_ver, d_vofs, d_err};
     const gjx::BatchSweep sw{d_mats, d_ks, d_cvg, d_done, d_swp, d_gs, d_gb, d_q, d_act, nmat};
-    const unsigned ctas =
-        std::min<unsigned>((width == gjx::kWidthHalf ? 2u : 1u) * (unsigned)sms, (unsigned)fitems.size());
+    const unsigned ctas = std::min<unsigned>((width >= gjx::kWidthHalf ? 2u : 1u) * (unsigned)sms,
+                                            (unsigned)(width == gjx::kWidthHalf2 ? (fitems.size() + 1u) / 2u
+                                                                                 : fitems.size()));
     for (unsigned k = 0u; k < kSweeps && ce == cudaSuccess; ++k) {
       ce = gjx::launch_batch_flow(cdsort, full, width, bf, ctas, st);
       if (ce == cudaSuccess)
@@ -694,8 +696,9 @@ int run_batch(const unsigned routine, const unsigned nmat, const unsigned *const
   cudaError_t ce = cudaSuccess;
   const gjx::BatchStep bs{d_mats, d_items, (unsigned)items.size(), d_ks, d_q, d_done, d_err};
   const gjx::BatchSweep sw{d_mats, d_ks, d_cvg, d_done, d_swp, d_gs, d_gb, d_q, d_act, nmat};
-  const unsigned ctas =
-      std::min<unsigned>((width == gjx::kWidthHalf ? 2u : 1u) * (unsigned)sms, (unsigned)items.size());
+  const unsigned ctas = std::min<unsigned>((width >= gjx::kWidthHalf ? 2u : 1u) * (unsigned)sms,
+                                          (unsigned)(width == gjx::kWidthHalf2 ? (items.size() + 1u) / 2u
+                                                                               : items.size()));
   for (unsigned k = 0u; k < kLaunches && ce == cudaSuccess; ++k) {
     ce = gjx::launch_batch_step(cdsort, full, width, bs, ctas, st);
     if (ce == cudaSuccess)
@@ -1295,7 +1298,7 @@ void gjx_set_variant(const unsigned v)
 void gjx_set_pairs_per_cta(const unsigned w)
 {
   std::lock_guard<std::mutex> lk(g_mtx);
-  g_pairs_per_cta = (w == 1u || w == 2u || w == gjx::kWidthHalf) ? w : 0u;
+  g_pairs_per_cta = (w >= 1u && w <= gjx::kWidthHalf2) ? w : 0u;
 }
 
 int gjx_autotune_batched(const unsigned routine, const unsigned nmat, const unsigned *const nrow,
@@ -1359,7 +1362,7 @@ int gjx_autotune_batched(const unsigned routine, const unsigned nmat, const unsi
   float best = 3.0e38f;
   std::pair<unsigned, int> pick{2u, 0};
   int rc = 0;
-  for (unsigned width : {2u, 1u, gjx::kWidthHalf}) {
+  for (unsigned width : {2u, 1u, gjx::kWidthHalf, gjx::kWidthHalf2}) {
     for (int mode : {0, 1}) {
       g_pairs_per_cta = width;
       g_batch_mode = mode;

@@ -96,8 +96,9 @@ cudaError_t launch_wait_selftest(long long limit, int *timed_out, long long *cyc
 bool sweep_kernel_fits(bool sort, bool accv, const StepParams &p);
 cudaError_t launch_l1_sweep(bool sort, bool accv, const StepParams &p, cudaStream_t s);
 // width 1: one block pair per CTA at a time; 2: two (pair_step2);
-// kWidthHalf: one per CTA of 4 warps, two CTAs per SM
-constexpr unsigned kWidthHalf = 3u;
+// kWidthHalf: one per CTA of 4 warps, two CTAs per SM; kWidthHalf2: two per
+// CTA of 4 warps, two CTAs per SM
+constexpr unsigned kWidthHalf = 3u, kWidthHalf2 = 4u;
 cudaError_t launch_batch_step(bool sort, bool accv, unsigned width, const BatchStep &b, unsigned ctas,
                               cudaStream_t s);
 cudaError_t launch_batch_sweep_end(const BatchSweep &w, cudaStream_t s);

@@ -654,6 +654,113 @@ __device__ __forceinline__ void inner_sweeps_q(double *const R, double *const Vl
   }
 }
 
+// by a group of 2 warps (lane x, warp w of the group, named barrier bar):
+// warp w takes pairs w, w + 2, ..., w + 14 of each inner step, and eighth k
+// of the warp (lanes 4k .. 4k + 3) computes pair w + 2k's rotation.  The
+// reduce-scatter of inner_sweeps_q goes one level further: at level 16 each
+// half keeps four pairs' products, at 8 each quarter two, at 4 each eighth
+// its own, levels 2 and 1 stay within the eighth -- the same operands in the
+// same order as the full butterfly.  Every lane then applies the eight
+// rotations to its row.
+template <bool SORT>
+__device__ __forceinline__ void inner_sweeps_e(double *const R, double *const Vl, const uint8_t *const s0,
+                                               const unsigned s0steps, const unsigned nswp, const int definite,
+                                               const unsigned npos, unsigned *const red, const unsigned x,
+                                               const unsigned w, const unsigned bar, unsigned &blk_s,
+                                               unsigned &blk_b)
+{
+  blk_s = 0u;
+  blk_b = 0u;
+  const bool up = x >= 16u, odd8 = ((x >> 3) & 1u) != 0u, odd4 = ((x >> 2) & 1u) != 0u;
+  const unsigned mine = w + 2u * (x >> 2); // the pair this lane's eighth evaluates
+  for (unsigned swp = 0u; swp < nswp; ++swp) {
+    unsigned ws = 0u, wb = 0u; // lanes 0, 4, ..., 28: their pairs' counts
+    for (unsigned step = 0u; step < s0steps; ++step) {
+      const uint8_t *const st = s0 + step * 32u;
+      unsigned p[8], q[8];
+      double Gp[8], Gq[8], Vp[8], Vq[8], v[8][3];
+#pragma unroll
+      for (unsigned k = 0u; k < 8u; ++k) {
+        p[k] = st[2u * (w + 2u * k)];
+        q[k] = st[2u * (w + 2u * k) + 1u];
+        Gp[k] = E32(R, x, p[k]);
+        Gq[k] = E32(R, x, q[k]);
+        Vp[k] = E32(Vl, x, p[k]);
+        Vq[k] = E32(Vl, x, q[k]);
+        v[k][0] = __fma_rn(Gp[k], Gp[k], 0.0);
+        v[k][1] = __fma_rn(Gq[k], Gq[k], 0.0);
+        v[k][2] = __fma_rn(Gp[k], Gq[k], 0.0);
+      }
+      const unsigned pm = st[2u * mine], qm = st[2u * mine + 1u];
+      double h4[4][3], h2[2][3], s[3];
+#pragma unroll
+      for (unsigned j = 0u; j < 4u; ++j)
+#pragma unroll
+        for (unsigned i = 0u; i < 3u; ++i) {
+          const double other = __shfl_xor_sync(0xffffffffu, up ? v[j][i] : v[4u + j][i], 16);
+          h4[j][i] = (up ? v[4u + j][i] : v[j][i]) + other;
+        }
+#pragma unroll
+      for (unsigned j = 0u; j < 2u; ++j)
+#pragma unroll
+        for (unsigned i = 0u; i < 3u; ++i) {
+          const double other = __shfl_xor_sync(0xffffffffu, odd8 ? h4[j][i] : h4[2u + j][i], 8);
+          h2[j][i] = (odd8 ? h4[2u + j][i] : h4[j][i]) + other;
+        }
+#pragma unroll
+      for (unsigned i = 0u; i < 3u; ++i) {
+        const double other = __shfl_xor_sync(0xffffffffu, odd4 ? h2[0][i] : h2[1][i], 4);
+        s[i] = (odd4 ? h2[1][i] : h2[0][i]) + other;
+      }
+#pragma unroll
+      for (unsigned k = 2u; k; k >>= 1u) {
+        double o[3];
+#pragma unroll
+        for (unsigned i = 0u; i < 3u; ++i)
+          o[i] = __shfl_xor_sync(0xffffffffu, s[i], k);
+#pragma unroll
+        for (unsigned i = 0u; i < 3u; ++i)
+          s[i] = s[i] + o[i];
+      }
+      unsigned a_s, a_b;
+      const Rot r = inner_rot<SORT>(s[0], s[1], s[2], pm, qm, definite, npos, a_s, a_b);
+      if (!(x & 3u)) {
+        ws += a_s;
+        wb += a_b;
+      }
+      const int fl = r.mode | (r.scale << 2) | (r.swap << 3);
+#pragma unroll
+      for (unsigned k = 0u; k < 8u; ++k) {
+        Rot o;
+        o.c = __shfl_sync(0xffffffffu, r.c, 4 * k);
+        o.t = __shfl_sync(0xffffffffu, r.t, 4 * k);
+        o.t_ = __shfl_sync(0xffffffffu, r.t_, 4 * k);
+        const int f = __shfl_sync(0xffffffffu, fl, 4 * k);
+        o.mode = f & 3;
+        o.scale = (f >> 2) & 1;
+        o.swap = (f >> 3) & 1;
+        inner_apply(R, Vl, p[k], q[k], o, x, Gp[k], Gq[k], Vp[k], Vq[k]);
+      }
+      bar_sync(bar, 64u);
+    }
+    ws = __reduce_add_sync(0xffffffffu, ws);
+    wb = __reduce_add_sync(0xffffffffu, wb);
+    if (x == 0u) {
+      red[2u * w] = ws;
+      red[2u * w + 1u] = wb;
+    }
+    bar_sync(bar, 64u);
+    const unsigned tot_s = red[0] + red[2], tot_b = red[1] + red[3];
+    bar_sync(bar, 64u);
+    if (tot_s) {
+      blk_s += tot_s;
+      blk_b += tot_b;
+    }
+    else
+      break;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Update of one 256-row stage: warp rg (0..7), lane = sub + 8*cg.  The thread
 // owns rows sub*32 + rg*4 + (0..3) and columns cg*8 + (0..7); entry (u, v)
@@ -1618,6 +1725,268 @@ __global__ void __launch_bounds__(kNThreads, 2) l1_batchn_kernel(const __grid_co
   }
 }
 
+// ---------------------------------------------------------------------------
+// Two block pairs on a CTA of 4 warps (batched form, two such CTAs per SM:
+// four pairs in flight per SM).  Pair A of matrix PA, pair B of matrix PB:
+// their Grams (gram_tile2 on warps 0-2, copies by warp 3) and updates (warp w
+// takes row groups w and w + 4 of every stage) run on the 4 warps, A's then
+// B's, as one stream of tiles and one of stages; their Cholesky
+// factorisations and inner sweeps run concurrently, warps 0-1 on A (named
+// barrier 1), warps 2-3 on B (barrier 2), with the eighth-warp reduce-scatter
+// of inner_sweeps_e.  Every entry gets the operations of pair_step in the
+// same order, so each matrix gets the bits of its single call.  Shared
+// memory (104 KB): the Gram's 4 stages of one tile, later one update buffer;
+// A's and B's R, V_loc and counters.
+// ---------------------------------------------------------------------------
+constexpr unsigned kN2OffRA = kNRegion;
+constexpr unsigned kN2OffVlA = kN2OffRA + 32u * kVTLd;
+constexpr unsigned kN2OffRB = kN2OffVlA + 1024u;
+constexpr unsigned kN2OffVlB = kN2OffRB + 32u * kVTLd;
+constexpr unsigned kN2OffS0 = kN2OffVlB + 1024u;
+constexpr unsigned kN2OffRed = kN2OffS0 + 128u; // [0..3] A's counts, [4..7] B's, [8..9] flags
+constexpr unsigned kN2OffBar = kN2OffRed + 8u;  // [0..3] Gram stages, [4] the update buffer
+constexpr unsigned kN2SmemDoubles = kN2OffBar + 8u;
+static_assert(2u * (kN2SmemDoubles * sizeof(double) + 1024u) <= 228u * 1024u, "two CTAs per SM");
+size_t batchn2_smem_bytes() { return (size_t)kN2SmemDoubles * sizeof(double); }
+
+template <bool SORT, bool ACCV>
+__device__ __forceinline__ void pair_step2n(const StepParams &PA, const unsigned stepA, const unsigned pairA,
+                                            const StepParams &PB, const unsigned stepB, const unsigned pairB,
+                                            double *const sm)
+{
+  double *const stg = sm;
+  uint8_t *const s0 = reinterpret_cast<uint8_t *>(sm + kN2OffS0);
+  unsigned *const red = reinterpret_cast<unsigned *>(sm + kN2OffRed);
+  uint64_t *const bars = reinterpret_cast<uint64_t *>(sm + kN2OffBar);
+  const unsigned tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+  size_t pidx = ((size_t)stepA * PA.pairs + pairA) * 2u;
+  const unsigned iA = PA.strat1[pidx + 0u], jA = PA.strat1[pidx + 1u];
+  pidx = ((size_t)stepB * PB.pairs + pairB) * 2u;
+  const unsigned iB = PB.strat1[pidx + 0u], jB = PB.strat1[pidx + 1u];
+
+  for (unsigned i = tid; i < 256u; i += kNThreads)
+    reinterpret_cast<uint32_t *>(s0)[i] = reinterpret_cast<const uint32_t *>(PA.strat0)[i];
+  if (tid == 0u) {
+    for (unsigned b = 0u; b < 5u; ++b)
+      mbar_init(&bars[b], 1u);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  // ------------------------------ 1. Grams --------------------------------
+  // tiles 0 .. ntA-1 are A's, ntA .. ntA+ntB-1 B's
+  const unsigned ntA = PA.nrow >> 6, ntB = PB.nrow >> 6, nt = ntA + ntB;
+  unsigned gx0 = 0u, gy = 0u, gy1 = 0u;
+  const bool gthr = gram_lane2(warp, lane, gx0, gy, gy1);
+  double gacc[4][2] = {{+0.0, +0.0}, {+0.0, +0.0}, {+0.0, +0.0}, {+0.0, +0.0}};
+  auto issue_gram = [&](const unsigned k) {
+    const unsigned s = k % kNGStages;
+    const bool a = k < ntA;
+    const CUtensorMap *const tm = a ? &PA.tmGram : &PB.tmGram;
+    const int tile = (int)(a ? k : (k - ntA));
+    double *const st = stg + s * kGramTileLd;
+    mbar_arrive_expect_tx(&bars[s], 2u * kGramBoxBytes);
+    tma_load_3d(st, tm, 0, tile, (int)((a ? iA : iB) * kNColB), &bars[s]);
+    tma_load_3d(st + 16u * kGramColLd, tm, 0, tile, (int)((a ? jA : jB) * kNColB), &bars[s]);
+  };
+  auto put_gram = [&](double *const R) { // our share of the lower triangle
+    if (gthr) {
+#pragma unroll
+      for (unsigned u = 0u; u < 4u; ++u)
+#pragma unroll
+        for (unsigned v = 0u; v < 2u; ++v) {
+          const unsigned y = v ? gy1 : gy;
+          if (gx0 + u >= y)
+            R[y * 32u + gx0 + u] = gacc[u][v];
+          gacc[u][v] = +0.0;
+        }
+    }
+  };
+  if (tid == kNIssuer)
+    for (unsigned k = 0u; k + 1u < kNGStages && k < nt; ++k)
+      issue_gram(k);
+  unsigned k = 0u;
+  int failed = 0;
+  for (; k < nt; ++k) {
+    if (tid == kNIssuer && k + kNGStages - 1u < nt)
+      issue_gram(k + kNGStages - 1u);
+    int fail = 0;
+    if (warp < 3u) {
+      if (!mbar_wait_bounded(&bars[k % kNGStages], (k / kNGStages) & 1u, kWaitLimit))
+        fail = 1;
+      else if (gthr)
+        gram_tile2(stg + (k % kNGStages) * kGramTileLd, 0u, gx0, gy, gy1, gacc);
+      if (k + 1u == ntA)
+        put_gram(sm + kN2OffRA);
+      else if (k + 1u == nt)
+        put_gram(sm + kN2OffRB);
+    }
+    failed = __syncthreads_or(fail);
+    if (failed)
+      break;
+  }
+  if (failed) {
+    if (tid == 0u) {
+      for (unsigned q = k; q < nt && q < k + kNGStages; ++q)
+        (void)mbar_wait_bounded(&bars[q % kNGStages], (q / kNGStages) & 1u, kWaitLimit / 8);
+      atomicOr(PA.err, kErrWaitTimeout);
+      atomicOr(PB.err, kErrWaitTimeout);
+    }
+    return;
+  }
+
+  // the update stages: A's, then B's; A's first one in flight during the
+  // serial phases
+  const unsigned nGA = (PA.nrow + kUpdRows - 1u) / kUpdRows, nGB = (PB.nrow + kUpdRows - 1u) / kUpdRows;
+  const unsigned nstA = nGA + (ACCV ? (PA.ncol + kUpdRows - 1u) / kUpdRows : 0u);
+  const unsigned nstB = nGB + (ACCV ? (PB.ncol + kUpdRows - 1u) / kUpdRows : 0u);
+  auto stage_at = [&](const unsigned g, const unsigned i, const CUtensorMap *&tm, int &piece) {
+    const StepParams &P = g ? PB : PA;
+    const unsigned nG = g ? nGB : nGA;
+    const bool isG = i < nG;
+    tm = isG ? &P.tmG : &P.tmV;
+    piece = (int)(((isG ? i : (i - nG)) * kUpdRows) >> 5);
+  };
+  auto issue_upd = [&](const unsigned g, const unsigned i) {
+    const CUtensorMap *tm;
+    int piece;
+    stage_at(g, i, tm, piece);
+    mbar_arrive_expect_tx(&bars[4], 2u * kUpdBoxBytes);
+    tma_load_3d(stg, tm, 0, piece, (int)((g ? iB : iA) * kNColB), &bars[4]);
+    tma_load_3d(stg + 16u * kUpdColLd, tm, 0, piece, (int)((g ? jB : jA) * kNColB), &bars[4]);
+  };
+  if (tid == 0u && nstA > 0u)
+    issue_upd(0u, 0u);
+
+  // ------------------- 2.-3. Cholesky and inner sweeps --------------------
+  {
+    const unsigned grp = warp >> 1, gt = tid & 63u, gw = warp & 1u;
+    const StepParams &P = grp ? PB : PA;
+    double *const R = sm + (grp ? kN2OffRB : kN2OffRA);
+    double *const Vl = sm + (grp ? kN2OffVlB : kN2OffVlA);
+    for (unsigned i = gt; i < 1024u; i += 64u)
+      Vl[i] = ((i >> 5) == (i & 31u)) ? 1.0 : 0.0;
+    chol32_grp<2u>(R, gt, 1u + grp);
+    bar_sync(1u + grp, 64u);
+    int definite;
+    unsigned npos;
+    block_signature(P, grp ? iB : iA, grp ? jB : jA, definite, npos);
+    unsigned blk_s, blk_b;
+    inner_sweeps_e<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red + 4u * grp, lane, gw, 1u + grp, blk_s,
+                         blk_b);
+    if (gt == 0u) {
+      add_counts(P, blk_s, blk_b);
+      red[8u + grp] = (SORT || blk_s) ? 1u : 0u;
+    }
+  }
+  __syncthreads();
+  const bool updA = red[8] != 0u, updB = red[9] != 0u;
+  // the stream of update stages: A's (or, when A is unchanged, its prefetched
+  // first stage, waited for and dropped), then B's
+  const unsigned qa = updA ? nstA : (nstA > 0u ? 1u : 0u), nq = qa + (updB ? nstB : 0u);
+  if (nq == qa && !updA) {
+    if (tid == 0u && qa > 0u && !mbar_wait_bounded(&bars[4], 0u, kWaitLimit))
+      atomicOr(PA.err, kErrWaitTimeout);
+    return;
+  }
+
+  // ------------------------------ 4. updates ------------------------------
+  for (unsigned i = tid; i < 2048u; i += kNThreads) { // both R are dead: B^T[s][c] = V_loc[s][c]
+    const unsigned g = i >> 10, c = (i >> 5) & 31u, s_ = i & 31u;
+    (sm + (g ? kN2OffRB : kN2OffRA))[s_ * kVTLd + c] = E32(sm + (g ? kN2OffVlB : kN2OffVlA), s_, c);
+  }
+  __syncthreads();
+  const unsigned sub = lane & 7u, cg8 = lane >> 3;
+  for (unsigned q = 0u; q < nq; ++q) {
+    const unsigned g = (q < qa) ? 0u : 1u, i = g ? q - qa : q;
+    if (tid == 0u && q > 0u) {
+      bulk_wait_read(); // the store of stage q - 1 has read the buffer out
+      issue_upd(g, i);
+    }
+    const int fail = !__all_sync(0xffffffffu, mbar_wait_bounded(&bars[4], q & 1u, kWaitLimit));
+    const bool work = g == 1u || updA;
+    if (!fail && work) {
+#pragma unroll 1
+      for (unsigned h = 0u; h < 2u; ++h) { // row groups warp and warp + 4
+        double acc[4][8];
+        update_stage(stg, sm + (g ? kN2OffRB : kN2OffRA), warp + 4u * h, sub, cg8, acc);
+        __syncwarp();
+        update_put(stg, acc, warp + 4u * h, sub, cg8);
+      }
+      fence_async_shared();
+    }
+    if (__syncthreads_or(fail)) {
+      if (tid == 0u) {
+        (void)mbar_wait_bounded(&bars[4], q & 1u, kWaitLimit / 8);
+        bulk_wait_all();
+        atomicOr(g ? PB.err : PA.err, kErrWaitTimeout);
+      }
+      return;
+    }
+    if (tid == 0u && work) {
+      const CUtensorMap *tm;
+      int piece;
+      stage_at(g, i, tm, piece);
+      tma_store_3d(tm, stg, 0, piece, (int)((g ? iB : iA) * kNColB));
+      tma_store_3d(tm, stg + 16u * kUpdColLd, 0, piece, (int)((g ? jB : jA) * kNColB));
+      bulk_commit();
+    }
+  }
+  if (tid == 0u)
+    bulk_wait_all();
+}
+
+// The batched step on CTAs of 4 warps, two per SM, two block pairs per CTA
+// at a time (items taken in twos from the queue, as l1_batch_kernel with W =
+// 2): two live pairs with the same inner table through pair_step2n, a lone
+// one through pair_step_n.  The mbarriers are invalidated after each item.
+template <bool SORT, bool ACCV>
+__global__ void __launch_bounds__(kNThreads, 2) l1_batchn2_kernel(const __grid_constant__ BatchStep B)
+{
+  extern __shared__ __align__(128) double sm[];
+  __shared__ unsigned item;
+  auto inval = [&](uint64_t *const bars) {
+    __syncthreads();
+    if (threadIdx.x == 0u)
+      for (unsigned k = 0u; k < 5u; ++k)
+        mbar_inval(&bars[k]);
+    __syncthreads();
+  };
+  for (;;) {
+    if (threadIdx.x == 0u)
+      item = atomicAdd(B.queue, 2u);
+    __syncthreads();
+    const unsigned it = item;
+    const bool stop = (it >= B.nitems) || (*(volatile int *)B.err != 0);
+    __syncthreads(); // every thread has read item
+    if (stop)
+      break;
+    const uint32_t e0 = B.items[it];
+    const bool live0 = !B.done[e0 >> 16u];
+    uint32_t e1 = 0u;
+    bool live1 = false;
+    if (it + 1u < B.nitems) {
+      e1 = B.items[it + 1u];
+      live1 = !B.done[e1 >> 16u];
+    }
+    if (live0 && live1 && B.mats[e0 >> 16u].p.strat0 == B.mats[e1 >> 16u].p.strat0) {
+      const BatchMat &ma = B.mats[e0 >> 16u], &mb = B.mats[e1 >> 16u];
+      pair_step2n<SORT, ACCV>(ma.p, B.kstep[e0 >> 16u] % ma.steps1, e0 & 0xffffu, mb.p,
+                              B.kstep[e1 >> 16u] % mb.steps1, e1 & 0xffffu, sm);
+      inval(reinterpret_cast<uint64_t *>(sm + kN2OffBar));
+      continue;
+    }
+    for (unsigned h = 0u; h < 2u; ++h) {
+      if (!(h ? live1 : live0))
+        continue;
+      const uint32_t e = h ? e1 : e0;
+      const BatchMat &m = B.mats[e >> 16u];
+      pair_step_n<SORT, ACCV>(m.p, B.kstep[e >> 16u] % m.steps1, e & 0xffffu, sm);
+      inval(reinterpret_cast<uint64_t *>(sm + kNOffBar));
+    }
+  }
+}
+
 // One launch per sweep of the whole batch (the dataflow form): the CTAs take
 // (matrix, step, pair) items in queue order -- step-major, every matrix's
 // step s before any step s + 1 -- and an item waits until both of its blocks
@@ -1789,6 +2158,117 @@ __global__ void __launch_bounds__(kNThreads, 2) l1_batchn_flow_kernel(const __gr
         mbar_inval(&bars[k]);
     }
     __syncthreads();
+  }
+}
+
+// The dataflow form on CTAs of 4 warps, two per SM, two items at a time:
+// two independent items (different matrices, or the same step, and the same
+// inner table) through pair_step2n, else one after the other through
+// pair_step_n; the readiness waits and write counts of l1_batch_flow_kernel.
+template <bool SORT, bool ACCV>
+__global__ void __launch_bounds__(kNThreads, 2) l1_batchn2_flow_kernel(const __grid_constant__ BatchFlow B)
+{
+  extern __shared__ __align__(128) double sm[];
+  __shared__ unsigned item, ok;
+  const unsigned tid = threadIdx.x;
+  auto blocks = [&](const uint32_t e, const unsigned stp, unsigned &iB, unsigned &jB) {
+    const BatchMat &m = B.mats[e >> 16u];
+    const size_t pidx = ((size_t)stp * m.p.pairs + (e & 0xffffu)) * 2u;
+    iB = m.p.strat1[pidx];
+    jB = m.p.strat1[pidx + 1u];
+  };
+  // thread 0: both blocks of the item written by its matrix's previous step (bounded)
+  auto ready = [&](const uint32_t e, const unsigned stp) -> bool {
+    unsigned iB, jB;
+    blocks(e, stp, iB, jB);
+    const unsigned *const v = B.ver + B.vofs[e >> 16u];
+    const long long t0 = clock64();
+    while (ld_acquire(v + iB) < stp || ld_acquire(v + jB) < stp) {
+      if (*(volatile int *)B.err)
+        return false;
+      if (clock64() - t0 > kWaitLimit) {
+        atomicOr(B.err, kErrWaitTimeout);
+        return false;
+      }
+      __nanosleep(64);
+    }
+    return true;
+  };
+  auto written = [&](const uint32_t e, const unsigned stp) { // thread 0, after the pair's stores completed
+    unsigned iB, jB;
+    blocks(e, stp, iB, jB);
+    unsigned *const v = B.ver + B.vofs[e >> 16u];
+    __threadfence();
+    atomicAdd(v + iB, 1u);
+    atomicAdd(v + jB, 1u);
+  };
+  auto inval = [&](uint64_t *const bars) {
+    __syncthreads();
+    if (tid == 0u)
+      for (unsigned k = 0u; k < 5u; ++k)
+        mbar_inval(&bars[k]);
+    __syncthreads();
+  };
+  for (;;) {
+    if (tid == 0u)
+      item = atomicAdd(B.queue, 2u);
+    __syncthreads();
+    const unsigned it = item;
+    const bool stop = (it >= B.nitems) || (*(volatile int *)B.err != 0);
+    __syncthreads();
+    if (stop)
+      break;
+    uint32_t e[2] = {B.items[it], 0u};
+    unsigned st[2] = {B.isteps[it], 0u};
+    bool live[2] = {!B.done[e[0] >> 16u], false};
+    if (it + 1u < B.nitems) {
+      e[1] = B.items[it + 1u];
+      st[1] = B.isteps[it + 1u];
+      live[1] = !B.done[e[1] >> 16u];
+    }
+    const unsigned b0 = e[0] >> 16u, b1 = e[1] >> 16u;
+    const bool both = live[0] && live[1] && (b0 != b1 || st[0] == st[1]) &&
+                      B.mats[b0].p.strat0 == B.mats[b1].p.strat0;
+    if (both) {
+      if (tid == 0u)
+        ok = ready(e[0], st[0]) && ready(e[1], st[1]);
+      __syncthreads();
+      if (!ok)
+        break;
+      asm volatile("fence.proxy.async;" ::: "memory"); // the copies below read what other SMs wrote
+      const BatchMat &ma = B.mats[b0], &mb = B.mats[b1];
+      pair_step2n<SORT, ACCV>(ma.p, st[0], e[0] & 0xffffu, mb.p, st[1], e[1] & 0xffffu, sm);
+      __threadfence();
+      __syncthreads();
+      if (tid == 0u) {
+        written(e[0], st[0]);
+        written(e[1], st[1]);
+      }
+      inval(reinterpret_cast<uint64_t *>(sm + kN2OffBar));
+      continue;
+    }
+    bool go = true;
+    for (unsigned h = 0u; h < 2u && go; ++h) {
+      if (!live[h])
+        continue;
+      if (tid == 0u)
+        ok = ready(e[h], st[h]);
+      __syncthreads();
+      if (!ok) {
+        go = false;
+        break;
+      }
+      asm volatile("fence.proxy.async;" ::: "memory");
+      const BatchMat &m = B.mats[e[h] >> 16u];
+      pair_step_n<SORT, ACCV>(m.p, st[h], e[h] & 0xffffu, sm);
+      __threadfence();
+      __syncthreads();
+      if (tid == 0u)
+        written(e[h], st[h]);
+      inval(reinterpret_cast<uint64_t *>(sm + kNOffBar));
+    }
+    if (!go)
+      break;
   }
 }
 
@@ -2076,6 +2556,9 @@ template <bool S, bool A> static cudaError_t set_smem_batch()
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(l1_batchn_kernel<S, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)batchn_smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(l1_batchn2_kernel<S, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)batchn2_smem_bytes());
   return e;
 }
 
@@ -2093,6 +2576,8 @@ static void batch_launch(const unsigned width, const BatchStep &b, const unsigne
 {
   if (width == kWidthHalf)
     l1_batchn_kernel<S, A><<<ctas, kNThreads, batchn_smem_bytes(), s>>>(b);
+  else if (width == kWidthHalf2)
+    l1_batchn2_kernel<S, A><<<ctas, kNThreads, batchn2_smem_bytes(), s>>>(b);
   else if (width == 2u)
     l1_batch_kernel<S, A, 2u><<<ctas, kThreads, batch2_smem_bytes(), s>>>(b);
   else
@@ -2125,8 +2610,12 @@ template <bool S, bool A> static cudaError_t set_smem_flow()
                            (int)batch2_smem_bytes());
   if (e != cudaSuccess)
     return e;
-  return cudaFuncSetAttribute(l1_batchn_flow_kernel<S, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)batchn_smem_bytes());
+  e = cudaFuncSetAttribute(l1_batchn_flow_kernel<S, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)batchn_smem_bytes());
+  if (e != cudaSuccess)
+    return e;
+  return cudaFuncSetAttribute(l1_batchn2_flow_kernel<S, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)batchn2_smem_bytes());
 }
 
 cudaError_t flow_configure()
@@ -2143,6 +2632,8 @@ static void flow_launch(const unsigned width, const BatchFlow &b, const unsigned
 {
   if (width == kWidthHalf)
     l1_batchn_flow_kernel<S, A><<<ctas, kNThreads, batchn_smem_bytes(), s>>>(b);
+  else if (width == kWidthHalf2)
+    l1_batchn2_flow_kernel<S, A><<<ctas, kNThreads, batchn2_smem_bytes(), s>>>(b);
   else if (width == 2u)
     l1_batch_flow_kernel<S, A, 2u><<<ctas, kThreads, batch2_smem_bytes(), s>>>(b);
   else

@@ -111,7 +111,9 @@ void gjx_set_split(unsigned n);
  * and inner sweeps of the two run concurrently on two groups of 4 warps), 1,
  * 3 (batched form only: one block pair per CTA of 4 warps, two such CTAs per
  * SM, so that one CTA's serial phases overlap the other's Gram and update),
- * or 0 (default): automatic -- the batched autotuner's
+ * 4 (batched form only: two block pairs per CTA of 4 warps, two such CTAs
+ * per SM; the two pairs' serial phases run concurrently on 2 warps each), or
+ * 0 (default): automatic -- the batched autotuner's
  * choice, else 2 in the batched form (gjx_hypJacL2_batched), and in the
  * per-step launches of a single matrix with one CTA per block pair when a
  * step has more block pairs than the GPU has SMs (one wave of CTAs instead of
@@ -150,7 +152,7 @@ void gjx_autotune_clear(void);
  * previous step.  The results are the same bits either way. */
 void gjx_set_batch_mode(int mode);
 
-/* Autotuner of the batched form: times block pairs per CTA (2, 1, 3) x launch
+/* Autotuner of the batched form: times block pairs per CTA (2, 1, 3, 4) x launch
  * mode (per step, per sweep) on seeded random matrices of the batch's shapes
  * (nrow[b] x ncol[b], the signature kind of nplus[b]), `sweeps` sweeps each
  * (0: 1), and uses the fastest in later gjx_hypJacL2_batched calls on a

@@ -2,7 +2,7 @@
 exactly what the single-matrix device call gives it -- U, V, D bit for bit,
 sweeps and rotation counts -- for mixed sizes (64..512 columns, square and
 tall), mixed signatures (J = I, J = -I, mixed), all four kernel variants
-(ALG 3, 9, 11, 1), one and two block pairs per CTA and one per CTA of 4 warps (two CTAs per SM), and a
+(ALG 3, 9, 11, 1), one and two block pairs per CTA of 8 warps and of 4 warps (two CTAs per SM), and a
 matrix with invalid arguments that is reported and left alone while the others run."""
 
 import numpy as np
@@ -30,12 +30,12 @@ CASES = [(64, 64, 64), (128, 128, 64), (192, 192, 0), (256, 256, 256), (320, 320
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("mode", [0, 1])
-@pytest.mark.parametrize("width", [2, 1, 3])
+@pytest.mark.parametrize("width", [2, 1, 3, 4])
 @pytest.mark.parametrize("alg", [11, 9, 3, 1])
 def test_batched_equals_single(built, alg, width, mode):
     import torch
     import gpujachx_b200 as g
-    g.lib().gjx_set_pairs_per_cta(width)   # 2: two block pairs per CTA, from different matrices too; 3: CTAs of 4 warps
+    g.lib().gjx_set_pairs_per_cta(width)   # 2 (4): two block pairs per CTA (of 4 warps), from different matrices too
     g.lib().gjx_set_batch_mode(mode)       # 0: one launch per step index, 1: one launch per sweep
     g.init_strats(None, "cycwor", 32, "cycwor", 4)   # the family; each matrix takes its own n1 table
     full = bool(alg & 2)
@@ -91,7 +91,7 @@ def test_batch_autotuner_picks_and_keeps_bits(built):
     shapes = [(128, 128, 128), (256, 256, 128), (192, 192, 0), (320, 320, 320), (128, 64, 64)]
     g.init_strats(None, "cycwor", 32, "cycwor", 4)
     pick = g.autotune_batched(11, [m for m, _, _ in shapes], [n for _, n, _ in shapes], [p for _, _, p in shapes])
-    assert pick["pairs_per_cta"] in (1, 2, 3) and pick["mode"] in (0, 1)
+    assert pick["pairs_per_cta"] in (1, 2, 3, 4) and pick["mode"] in (0, 1)
     mats = [synth.make("svd_synth", m, n, 7000 + k, smin=1e-6) if m == n else synth.make("graded", m, n, 7000 + k)
             for k, (m, n, _) in enumerate(shapes)]
     batch = [_dev(G, True) for G in mats]
