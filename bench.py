@@ -474,7 +474,12 @@ def main_batch(args):
     g.init_strats(None, "cycwor", 32, "cycwor", 4)
     # the library's batched autotuner, once per batch shape, before timing:
     # block pairs per CTA and one launch per step index or per sweep
-    tuned = g.autotune_batched(ALG, [int(n) for n in sizes], [int(n) for n in sizes], nplus)
+    if args.pairs_per_cta:  # a fixed form (profiling runs): per-step launches of that form, no tuning
+        g.lib().gjx_set_pairs_per_cta(args.pairs_per_cta)
+        g.lib().gjx_set_batch_mode(0)
+        tuned = {"pairs_per_cta": args.pairs_per_cta, "mode": 0}
+    else:
+        tuned = g.autotune_batched(ALG, [int(n) for n in sizes], [int(n) for n in sizes], nplus)
     width = tuned["pairs_per_cta"]
     dG = torch.empty_like(G0)
     dV = torch.empty_like(G0)
@@ -735,6 +740,8 @@ def main():
     ap.add_argument("--accuracy", action="store_true", help="add pp80 figures of the last decomposition")
     ap.add_argument("--shard", action="store_true", help="c5 over N ranks: split one batch instead of N batches")
     ap.add_argument("--count", type=int, default=0, help="c5: matrices in the batch (default 4096; profiling runs)")
+    ap.add_argument("--pairs-per-cta", type=int, default=0, choices=[0, 1, 2, 3, 4],
+                    help="c5: fix the batched form (per-step launches) instead of the autotuner's pick")
     ap.add_argument("--alg", type=int, default=-1, help="override the workload's ALG (studies; the config says so)")
     ap.add_argument("--form", default="plain", choices=["plain", "split"],
                     help="plain FP64 (the drop-in) or the split-precision form (gjx_hypJacL2_split)")
