@@ -109,11 +109,16 @@ static __device__ __noinline__ double rsqrt_rn_full(const double a)
 // Fast path: the estimate from the hardware approximation (relative error
 // about 2^-20, measured) refined by one second-order Newton step to about
 // an ulp, then the same rounding decision as rsqrt_rn_full (after Markstein).
-// Powers of 4 (f = 1) give 2^-kk exactly.  Whatever the decision cannot
-// settle -- signs, zeros, subnormals, inf, NaN and the rare ambiguous
-// roundings -- goes to rsqrt_rn_full in one branch at the end (the fast
-// path's values for those inputs are discarded), so the result is the
-// correctly rounded 1/sqrt(a) either way.
+// The residual e = 1 - f y^2 is formed from a and the unscaled estimate ya
+// (f y^2 = a ya^2: the power-of-4 scalings cancel), so the scaling of y into
+// (1/2, 1] runs beside it; Y = rint(y 2^53 + d) comes from one FMA whose
+// result lies in [2^52, 2^53), where doubles are the integers.  Powers of 4
+// (f = 1) give 2^-kk exactly.  Whatever the decision cannot settle -- signs,
+// zeros, subnormals, inf, NaN, exponents beyond +-960 (where a ya^2 could
+// leave the normal range) and the rare ambiguous roundings -- goes to
+// rsqrt_rn_full in one branch at the end (the fast path's values for those
+// inputs are discarded), so the result is the correctly rounded 1/sqrt(a)
+// either way.
 __device__ __forceinline__ double rsqrt_rn(const double a)
 {
   const unsigned long long bits = (unsigned long long)__double_as_longlong(a);
@@ -124,22 +129,22 @@ __device__ __forceinline__ double rsqrt_rn(const double a)
   const double r0 = __fma_rn(-h0, y0, 1.0);
   const double ya = __fma_rn(y0 * r0, __fma_rn(0.375, r0, 0.5), y0); // y0 (1 + r0/2 + 3 r0^2/8)
   const int eu = (int)ef - 1023;
-  const int k2 = eu & ~1;
-  const double f = __longlong_as_double((long long)((bits & 0xFFFFFFFFFFFFFull) | ((unsigned long long)(1023 + (eu - k2)) << 52)));
-  const int kk = k2 / 2;
-  const double y = ya * pow2(kk);
-  const double yh = y * y;
-  const double yl = __fma_rn(y, y, -yh);
-  const double e = __fma_rn(-f, yl, __fma_rn(-f, yh, 1.0));
-  // (y (e/2)) 2^53 of rsqrt_rn_full, the same bits: scalings by powers of 2 are exact
-  const double d = (y * e) * pow2(52);
-  // rint(d) for |d| < 2^51 (round to nearest even by the addition)
-  const double dr = (d + 0x1.8p52) - 0x1.8p52;
-  const double Yd = __fma_rn(y, pow2(53), dr);
+  const int kk = (eu & ~1) / 2; // a = f * 4^kk, f in [1, 4)
+  // e = 1 - f y^2 with y^2 = yh + yl split exactly (y = ya 2^kk, f = a 4^-kk)
+  const double yh = ya * ya;
+  const double yl = __fma_rn(ya, ya, -yh);
+  const double e = __fma_rn(-a, yl, __fma_rn(-a, yh, 1.0));
+  const double y52 = ya * pow2(52 + kk); // y 2^52 (exact), beside the residual
+  // the correction in ulps of y, (y (e/2)) 2^53 = (y 2^52) e
+  const double d = y52 * e;
+  // Y = y 2^53 + rint(d): y 2^53 is an integer, and the FMA rounds the sum
+  // in [2^52, 2^53) to an integer (ties cannot occur: they are refused below)
+  const double Yd = __fma_rn(y52, 2.0, d);
+  const double dr = Yd - 2.0 * y52; // rint(d), exact
   // a power of 4 (f = 1, e.g. 1 + t^2 = 1 for a tiny rotation angle): 2^-kk exactly
-  const bool p4 = (f == 1.0);
+  const bool p4 = !(bits & 0xFFFFFFFFFFFFFull) && !(eu & 1);
   const double res = p4 ? pow2(-kk) : Yd * pow2(-53 - kk);
-  if ((ef - 1ull > 2045ull) ||
+  if ((ef - 1ull > 2045ull) || (eu < -960) || (eu > 960) ||
       (!p4 && (!(fabs(d) < 0x1.0p50) || fabs(d - dr) > 0.5 - 0x1.0p-40 || Yd >= pow2(53) || Yd < pow2(52))))
     return rsqrt_rn_full(a);
   return res;
