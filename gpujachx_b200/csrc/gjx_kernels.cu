@@ -370,10 +370,27 @@ __device__ __forceinline__ void chol32_grp(double *const R, const unsigned gt, c
       chol_pivot(R, j, x, a);
     }
     else {
+      // the columns of a round are independent: four at a time, so that
+      // their shared-memory loads overlap (each entry's operations unchanged)
+      const double xk = -E32(R, x, k);
+      unsigned j = k + 1u + w;
 #pragma unroll 1
-      for (unsigned j = k + 1u + w; j < 32u; j += NW - 1u)
+      for (; j + 3u * (NW - 1u) < 32u; j += 4u * (NW - 1u)) {
+        double ajk[4], axj[4];
+#pragma unroll
+        for (unsigned u = 0u; u < 4u; ++u) {
+          ajk[u] = E32(R, j + u * (NW - 1u), k);
+          axj[u] = E32(R, x, j + u * (NW - 1u));
+        }
+#pragma unroll
+        for (unsigned u = 0u; u < 4u; ++u)
+          if (x >= j + u * (NW - 1u))
+            E32(R, x, j + u * (NW - 1u)) = __fma_rn(xk, ajk[u], axj[u]);
+      }
+#pragma unroll 1
+      for (; j < 32u; j += NW - 1u)
         if (x >= j)
-          E32(R, x, j) = __fma_rn(-E32(R, x, k), E32(R, j, k), E32(R, x, j));
+          E32(R, x, j) = __fma_rn(xk, E32(R, j, k), E32(R, x, j));
     }
     bar_sync(bar, NW * 32u);
   }
