@@ -207,9 +207,35 @@ struct Rot {
   int scale, swap;
 };
 
-// rotT (trig) or rotH; when the two halves of the warp need different kinds,
-// both are computed and selected, so the warp does not run them one after
-// the other (each is a long dependent chain of divisions and square roots)
+// rotT for the lanes with trig, rotH for the others, in one chain.  The two
+// formulas take the same operations up to signs -- Dq - Dp is Dq + (-Dp)
+// exactly, the quotient negated, +1 or -1 under the square root, t t + 1 or
+// -t t + 1 under the reciprocal square root -- and their special cases are
+// selects, so each lane gets exactly the operations of its own formula while
+// a warp whose lanes need both kinds runs one chain of divides and square
+// roots instead of two.
+__device__ __forceinline__ int rotTH(const bool trig, const double Apq, const double Dp, const double Dq, double &c,
+                                     double &t)
+{
+  const double h = Dq + (trig ? -Dp : Dp);
+  const double qt = __ddiv_rn(h, Apq * 2.0);
+  const double ct2 = trig ? qt : -qt;
+  const double CT2 = fabs(ct2);
+  const bool large = CT2 >= kSqrt2Heps;
+  const bool small = trig && (CT2 < kSqrtHeps);      // rotT's first case
+  const bool mid = !trig && !large && (CT2 > 1.0);  // rotH's middle case
+  const double cot_mid = CT2 + __dsqrt_rn(__fma_rn(CT2, CT2, trig ? 1.0 : -1.0));
+  const double cot = small ? (CT2 + 1.0) : (large ? (CT2 * 2.0) : cot_mid);
+  const double tt = copysign(__drcp_rn(cot), ct2);
+  const double cr = rsqrt_rn(__fma_rn(trig ? tt : -tt, tt, 1.0));
+  c = large ? 1.0 : ((trig || mid) ? cr : kCoshIFix);
+  t = (trig || large || mid) ? tt : kTanh1Fix;
+  return trig ? (small ? 1 : (large ? 0 : (cr < 1.0))) : (large ? 0 : (mid ? (cr > 1.0) : 1));
+}
+
+// rotT (trig) or rotH; when the lanes of the warp need different kinds, the
+// merged chain of rotTH (each is a long dependent chain of divisions and
+// square roots)
 __device__ __forceinline__ int rot_either(const bool trig, const double Apq, const double Dp, const double Dq,
                                           double &c, double &t)
 {
@@ -217,11 +243,7 @@ __device__ __forceinline__ int rot_either(const bool trig, const double Apq, con
     return rotT(Apq, Dp, Dq, c, t);
   if (__all_sync(0xffffffffu, !trig))
     return rotH(Apq, Dp, Dq, c, t);
-  double c1, t1, c2, t2;
-  const int b1 = rotT(Apq, Dp, Dq, c1, t1), b2 = rotH(Apq, Dp, Dq, c2, t2);
-  c = trig ? c1 : c2;
-  t = trig ? t1 : t2;
-  return trig ? b1 : b2;
+  return rotTH(trig, Apq, Dp, Dq, c, t);
 }
 
 template <bool SORT>
