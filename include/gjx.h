@@ -231,8 +231,11 @@ int gjx_hypJacL2_dev(const unsigned routine, const unsigned nrow, const unsigned
  * GJX_ERR_SCRATCH.  The first call on a device takes the array's address
  * (cudaGetSymbolAddress) with that device current; make it before any stream
  * capture.  All calls share the array: each clears its counters and rewrites
- * the tables when they or the device changed; calls that overlap on the GPU
- * race.  Same arguments, results and other codes as gjx_hypJacL2_dev.
+ * the tables when they or the device changed (or the device's context was
+ * re-created); calls that overlap on the GPU race.  The call holds the
+ * library's host lock until its result is ready, so other calls into the
+ * library from the same process wait for it.  Same arguments, results and
+ * other codes as gjx_hypJacL2_dev.
  */
 int gjx_hypJacL2_noalloc(const unsigned routine, const unsigned nrow, const unsigned ncol, const unsigned nplus,
                          double *const dG, const unsigned lddG, double *const dV, const unsigned lddV,
