@@ -574,12 +574,15 @@ __device__ __forceinline__ void inner_sweeps(double *const R, double *const Vl, 
 // quarter its own pair's, levels 4, 2, 1 stay within the quarter -- the same
 // operands in the same order as the full butterfly, with one rotation to
 // evaluate per warp and step.  Every lane then applies the four rotations.
+// The four rotations of a warp reach its lanes through shared memory (rs: 16
+// doubles of this warp's own; the lane 8k writes pair k's, every lane reads
+// all four back with broadcast loads), not through shuffles.
 template <bool SORT>
 __device__ __forceinline__ void inner_sweeps_q(double *const R, double *const Vl, const uint8_t *const s0,
                                                const unsigned s0steps, const unsigned nswp, const int definite,
                                                const unsigned npos, unsigned *const red, const unsigned x,
                                                const unsigned w, const unsigned bar, unsigned &blk_s,
-                                               unsigned &blk_b)
+                                               unsigned &blk_b, double *const rs)
 {
   blk_s = 0u;
   blk_b = 0u;
@@ -632,15 +635,22 @@ __device__ __forceinline__ void inner_sweeps_q(double *const R, double *const Vl
       if (!(x & 7u)) {
         ws += a_s;
         wb += a_b;
+        double *const e = rs + 4u * (x >> 3);
+        e[0] = r.c;
+        e[1] = r.t;
+        e[2] = r.t_;
+        e[3] = __longlong_as_double((long long)(r.mode | (r.scale << 2) | (r.swap << 3)));
       }
-      const int fl = r.mode | (r.scale << 2) | (r.swap << 3);
+      __syncwarp();
 #pragma unroll
       for (unsigned k = 0u; k < 4u; ++k) {
+        const double2 ct = *reinterpret_cast<const double2 *>(rs + 4u * k);
+        const double2 tf = *reinterpret_cast<const double2 *>(rs + 4u * k + 2u);
         Rot o;
-        o.c = __shfl_sync(0xffffffffu, r.c, 8 * k);
-        o.t = __shfl_sync(0xffffffffu, r.t, 8 * k);
-        o.t_ = __shfl_sync(0xffffffffu, r.t_, 8 * k);
-        const int f = __shfl_sync(0xffffffffu, fl, 8 * k);
+        o.c = ct.x;
+        o.t = ct.y;
+        o.t_ = tf.x;
+        const int f = (int)__double_as_longlong(tf.y);
         o.mode = f & 3;
         o.scale = (f >> 2) & 1;
         o.swap = (f >> 3) & 1;
@@ -679,12 +689,15 @@ __device__ __forceinline__ void inner_sweeps_q(double *const R, double *const Vl
 // its own, levels 2 and 1 stay within the eighth -- the same operands in the
 // same order as the full butterfly.  Every lane then applies the eight
 // rotations to its row.
+// The eight rotations of a warp reach its lanes through shared memory (rs:
+// 32 doubles of this warp's own; lane 4k writes pair k's), as in
+// inner_sweeps_q.
 template <bool SORT>
 __device__ __forceinline__ void inner_sweeps_e(double *const R, double *const Vl, const uint8_t *const s0,
                                                const unsigned s0steps, const unsigned nswp, const int definite,
                                                const unsigned npos, unsigned *const red, const unsigned x,
                                                const unsigned w, const unsigned bar, unsigned &blk_s,
-                                               unsigned &blk_b)
+                                               unsigned &blk_b, double *const rs)
 {
   blk_s = 0u;
   blk_b = 0u;
@@ -744,15 +757,22 @@ __device__ __forceinline__ void inner_sweeps_e(double *const R, double *const Vl
       if (!(x & 3u)) {
         ws += a_s;
         wb += a_b;
+        double *const e = rs + 4u * (x >> 2);
+        e[0] = r.c;
+        e[1] = r.t;
+        e[2] = r.t_;
+        e[3] = __longlong_as_double((long long)(r.mode | (r.scale << 2) | (r.swap << 3)));
       }
-      const int fl = r.mode | (r.scale << 2) | (r.swap << 3);
+      __syncwarp();
 #pragma unroll
       for (unsigned k = 0u; k < 8u; ++k) {
+        const double2 ct = *reinterpret_cast<const double2 *>(rs + 4u * k);
+        const double2 tf = *reinterpret_cast<const double2 *>(rs + 4u * k + 2u);
         Rot o;
-        o.c = __shfl_sync(0xffffffffu, r.c, 4 * k);
-        o.t = __shfl_sync(0xffffffffu, r.t, 4 * k);
-        o.t_ = __shfl_sync(0xffffffffu, r.t_, 4 * k);
-        const int f = __shfl_sync(0xffffffffu, fl, 4 * k);
+        o.c = ct.x;
+        o.t = ct.y;
+        o.t_ = tf.x;
+        const int f = (int)__double_as_longlong(tf.y);
         o.mode = f & 3;
         o.scale = (f >> 2) & 1;
         o.swap = (f >> 3) & 1;
@@ -1129,7 +1149,8 @@ __device__ __forceinline__ void pair_step(const StepParams &P, const unsigned st
 constexpr unsigned kOffR2 = kSmemDoubles; // pair B's R (later B^T), V_loc, counters
 constexpr unsigned kOffVl2 = kOffR2 + 32u * kVTLd;
 constexpr unsigned kOffRed2 = kOffVl2 + 1024u;
-constexpr unsigned kSmemDoubles2 = kOffRed2 + 16u;
+constexpr unsigned kOffRot2 = kOffRed2 + 16u; // the rotations of the 8 warps (inner_sweeps_q), 16 doubles each
+constexpr unsigned kSmemDoubles2 = kOffRot2 + 128u;
 
 size_t batch2_smem_bytes() { return (size_t)kSmemDoubles2 * sizeof(double); }
 
@@ -1290,7 +1311,8 @@ __device__ __forceinline__ void pair_step2(const StepParams &PA, const unsigned 
     unsigned npos;
     block_signature(P, grp ? iB : iA, grp ? jB : jA, definite, npos);
     unsigned blk_s, blk_b;
-    inner_sweeps_q<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, lane, gw, 1u + grp, blk_s, blk_b);
+    inner_sweeps_q<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, lane, gw, 1u + grp, blk_s, blk_b,
+                         sm + kOffRot2 + 16u * warp);
     if (gt == 0u) {
       add_counts(P, blk_s, blk_b);
       flags[grp] = (SORT || blk_s) ? 1u : 0u;
@@ -1555,7 +1577,8 @@ constexpr unsigned kNOffVl = kNOffR + 32u * kVTLd;
 constexpr unsigned kNOffS0 = kNOffVl + 1024u;
 constexpr unsigned kNOffRed = kNOffS0 + 128u;
 constexpr unsigned kNOffBar = kNOffRed + 16u; // [0..3] Gram stages, [4] the update buffer
-constexpr unsigned kNSmemDoubles = kNOffBar + 8u;
+constexpr unsigned kNOffRot = kNOffBar + 8u; // the rotations of the 4 warps (inner_sweeps_q), 16 doubles each
+constexpr unsigned kNSmemDoubles = kNOffRot + 64u;
 static_assert(2u * (kNSmemDoubles * sizeof(double) + 1024u) <= 228u * 1024u, "two CTAs per SM");
 size_t batchn_smem_bytes() { return (size_t)kNSmemDoubles * sizeof(double); }
 
@@ -1657,7 +1680,8 @@ __device__ __forceinline__ void pair_step_n(const StepParams &P, const unsigned 
   unsigned npos;
   block_signature(P, iBlk, jBlk, definite, npos);
   unsigned blk_s, blk_b;
-  inner_sweeps_q<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, lane, warp, 0u, blk_s, blk_b);
+  inner_sweeps_q<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, lane, warp, 0u, blk_s, blk_b,
+                       sm + kNOffRot + 16u * warp);
   if (tid == 0u)
     add_counts(P, blk_s, blk_b);
   if (!SORT && !blk_s) { // no rotation: the block pair is unchanged
@@ -1762,7 +1786,8 @@ constexpr unsigned kN2OffVlB = kN2OffRB + 32u * kVTLd;
 constexpr unsigned kN2OffS0 = kN2OffVlB + 1024u;
 constexpr unsigned kN2OffRed = kN2OffS0 + 128u; // [0..3] A's counts, [4..7] B's, [8..9] flags
 constexpr unsigned kN2OffBar = kN2OffRed + 8u;  // [0..3] Gram stages, [4] the update buffer
-constexpr unsigned kN2SmemDoubles = kN2OffBar + 8u;
+constexpr unsigned kN2OffRot = kN2OffBar + 8u; // the rotations of the 4 warps (inner_sweeps_e), 32 doubles each
+constexpr unsigned kN2SmemDoubles = kN2OffRot + 128u;
 static_assert(2u * (kN2SmemDoubles * sizeof(double) + 1024u) <= 228u * 1024u, "two CTAs per SM");
 size_t batchn2_smem_bytes() { return (size_t)kN2SmemDoubles * sizeof(double); }
 
@@ -1890,7 +1915,7 @@ __device__ __forceinline__ void pair_step2n(const StepParams &PA, const unsigned
     block_signature(P, grp ? iB : iA, grp ? jB : jA, definite, npos);
     unsigned blk_s, blk_b;
     inner_sweeps_e<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red + 4u * grp, lane, gw, 1u + grp, blk_s,
-                         blk_b);
+                         blk_b, sm + kN2OffRot + 32u * warp);
     if (gt == 0u) {
       add_counts(P, blk_s, blk_b);
       red[8u + grp] = (SORT || blk_s) ? 1u : 0u;
