@@ -110,7 +110,9 @@ def build_strat(ref_root: str | None = None, force: bool = False, verbose: bool 
 
     The headers are data (``unsigned char|short <family>NNNNN[S][N/2][2] = {...}``);
     they are consumed unchanged, as the reference's own strat/proc_*-lnx.sh
-    does, with the same exported symbol names.
+    does, with the same exported symbol names.  The rowcyc and colcyc tables
+    of orders 960 and 1024, which the reference does not ship, are added by
+    its doubling construction (strat_gen).
     """
     ref_root = ref_root or os.environ.get("GJX_REF_ROOT", "")
     sdir = os.path.join(ref_root, "strat") if ref_root else ""
@@ -135,8 +137,19 @@ def build_strat(ref_root: str | None = None, force: bool = False, verbose: bool 
             subprocess.check_call(["gcc", "-O0", "-fPIC", "-c", "-o", o, c])
             return o
 
+        def ext(item):  # the tables beyond the reference's largest order (strat_gen)
+            name, src = item
+            c = os.path.join(work, name)
+            with open(c, "w") as f:
+                f.write(src)
+            o = c[:-2] + ".o"
+            subprocess.check_call(["gcc", "-O0", "-fPIC", "-c", "-o", o, c])
+            return o
+
+        from . import strat_gen
         with ThreadPoolExecutor(max_workers=len(STRAT_FAMILIES)) as ex:
             objs = list(ex.map(one, STRAT_FAMILIES))
+            objs += list(ex.map(ext, sorted(strat_gen.extension_sources(sdir).items())))
         tmp = STRAT + ".tmp"
         _run(["gcc", "-shared", "-o", tmp] + objs, verbose)
         os.replace(tmp, STRAT)

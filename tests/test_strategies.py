@@ -29,8 +29,12 @@ def _orders(strat_path):
 
 def test_table_count(strat_path):
     o = _orders(strat_path)
-    assert len(o) == 325  # every shipped header; 00960 and 01024 are absent upstream
-    assert max(n for _, n in o) == 896
+    # every shipped header (orders up to 896), and the rowcyc / colcyc tables
+    # of orders 960 and 1024 that the build adds by the doubling construction
+    assert len(o) == 325 + 4
+    assert max(n for _, n in o) == 1024
+    assert sorted(x for x in o if x[1] > 896) == [("colcyc", 960), ("colcyc", 1024), ("rowcyc", 960),
+                                                  ("rowcyc", 1024)]
 
 
 def test_every_table_is_a_parallel_ordering(strat_path, oracle):
@@ -71,7 +75,7 @@ def test_strategy_ids(built):
 
 
 def test_validator_accepts_every_shipped_table(built):
-    """gjx_validate_pairs on all tables up to n1 = 1024: perfect matchings,
+    """gjx_validate_pairs on all tables (up to n1 = 1024): perfect matchings,
     full coverage; repeats only in mmstep (n/2 pairs twice, n steps)."""
     import re
     import subprocess
@@ -79,7 +83,7 @@ def test_validator_accepts_every_shipped_table(built):
     from oracle import oracle
     syms = subprocess.run(["nm", "-D", "--defined-only", built["strat"]], capture_output=True, text=True).stdout.split()
     names = sorted({s for s in syms if re.fullmatch(r"[A-Za-z]+\d{5}", s)})
-    assert len(names) == 325
+    assert len(names) == 325 + 4  # and the added rowcyc / colcyc of orders 960, 1024
     for nm in names:
         fam, n = nm[:-5], int(nm[-5:])
         t = oracle.load_strat(built["strat"], fam, n)
