@@ -293,7 +293,8 @@ constexpr uint32_t kOffRed = kOffScale + 512u;                               // 
 constexpr uint32_t kOffBar = kOffRed + 256u;                                 // 8 mbarriers
 constexpr uint32_t kOffTmem = kOffBar + 64u;
 static_assert(kGStages + 2u <= 8u, "stage and plane-buffer mbarriers must fit their region");
-constexpr uint32_t kPairSmem = kOffTmem + 16u;
+constexpr uint32_t kOffRot = kOffTmem + 16u;                                 // 8 warps x 16 doubles: rotations
+constexpr uint32_t kPairSmem = kOffRot + 1024u;
 static_assert(kPairSmem <= 227u * 1024u, "shared memory of sp_pair_kernel");
 
 __device__ __forceinline__ void set_err(const Params &P) { atomicExch(P.err, kErrWaitTimeout); }
@@ -333,11 +334,16 @@ __device__ __forceinline__ void pair_signature(const Params &P, const unsigned i
 // the inner sweep(s) on R (64 x 64) accumulating V_loc: per inner step warp w
 // takes pairs 4w .. 4w + 3; lane x holds rows x and x + 32; quarter c of the
 // warp (lanes 8c .. 8c + 7) evaluates pair 4w + c's rotation, every lane
-// applies all four.  One barrier per step.
+// applies all four.  The twelve sums go through a reduce-scatter (at level 16
+// each half keeps its two pairs' products, at level 8 each quarter its own,
+// levels 4, 2, 1 within the quarter: the same operands in the same order as
+// the full butterfly, with 18 shuffles instead of 60), and the four rotations
+// reach every lane through rs (16 doubles of this warp's own shared memory;
+// lane 8c writes pair c's), not through shuffles.  One barrier per step.
 template <bool SORT>
 __device__ void inner64(double *const R, double *const Vl, const uint8_t *const s0, const unsigned s0steps,
                         const unsigned nswp, const int definite, const unsigned npos, unsigned *const red,
-                        unsigned &blk_s, unsigned &blk_b)
+                        unsigned &blk_s, unsigned &blk_b, double *const rs)
 {
   const unsigned tid = threadIdx.x, x = tid & 31u, w = tid >> 5;
   blk_s = 0u;
@@ -365,38 +371,54 @@ __device__ void inner64(double *const R, double *const Vl, const uint8_t *const 
         d[c][1] = __fma_rn(gq1[c], gq1[c], gq0[c] * gq0[c]);
         d[c][2] = __fma_rn(gp1[c], gq1[c], gp0[c] * gq0[c]);
       }
+      const bool up = x >= 16u, odd = ((x >> 3) & 1u) != 0u;
+      double h[2][3], sm3[3];
 #pragma unroll
-      for (unsigned o = 16u; o; o >>= 1u)
+      for (unsigned j = 0u; j < 2u; ++j)
 #pragma unroll
-        for (unsigned c = 0u; c < 4u; ++c)
+        for (unsigned i = 0u; i < 3u; ++i) {
+          const double other = __shfl_xor_sync(0xffffffffu, up ? d[j][i] : d[2u + j][i], 16);
+          h[j][i] = (up ? d[2u + j][i] : d[j][i]) + other;
+        }
 #pragma unroll
-          for (unsigned i = 0u; i < 3u; ++i)
-            d[c][i] += __shfl_xor_sync(0xffffffffu, d[c][i], o);
+      for (unsigned i = 0u; i < 3u; ++i) {
+        const double other = __shfl_xor_sync(0xffffffffu, odd ? h[0][i] : h[1][i], 8);
+        sm3[i] = (odd ? h[1][i] : h[0][i]) + other;
+      }
+#pragma unroll
+      for (unsigned o = 4u; o; o >>= 1u)
+#pragma unroll
+        for (unsigned i = 0u; i < 3u; ++i)
+          sm3[i] += __shfl_xor_sync(0xffffffffu, sm3[i], o);
       const unsigned mc = x >> 3; // this lane's pair among the warp's four
-      double Dp = d[0][0], Dq = d[0][1], Apq = d[0][2];
       unsigned pm = p[0], qm = q[0];
 #pragma unroll
       for (unsigned c = 1u; c < 4u; ++c)
         if (mc == c) {
-          Dp = d[c][0];
-          Dq = d[c][1];
-          Apq = d[c][2];
           pm = p[c];
           qm = q[c];
         }
       unsigned a_s = 0u, a_b = 0u;
-      const Rot mine = inner_rot<SORT>(Dp, Dq, Apq, pm, qm, definite, npos, a_s, a_b);
+      const Rot mine = inner_rot<SORT>(sm3[0], sm3[1], sm3[2], pm, qm, definite, npos, a_s, a_b);
       if ((x & 7u) == 0u) {
         ws += a_s;
         wb += a_b;
+        double *const e = rs + 4u * mc;
+        e[0] = mine.c;
+        e[1] = mine.t;
+        e[2] = mine.t_;
+        e[3] = __longlong_as_double((long long)(mine.mode | (mine.scale << 2) | (mine.swap << 3)));
       }
+      __syncwarp();
 #pragma unroll
       for (unsigned c = 0u; c < 4u; ++c) {
+        const double2 ct = *reinterpret_cast<const double2 *>(rs + 4u * c);
+        const double2 tf = *reinterpret_cast<const double2 *>(rs + 4u * c + 2u);
         Rot r;
-        r.c = __shfl_sync(0xffffffffu, mine.c, 8u * c);
-        r.t = __shfl_sync(0xffffffffu, mine.t, 8u * c);
-        r.t_ = __shfl_sync(0xffffffffu, mine.t_, 8u * c);
-        const int fl = __shfl_sync(0xffffffffu, mine.mode | (mine.scale << 2) | (mine.swap << 3), 8u * c);
+        r.c = ct.x;
+        r.t = ct.y;
+        r.t_ = tf.x;
+        const int fl = (int)__double_as_longlong(tf.y);
         r.mode = fl & 3;
         r.scale = (fl >> 2) & 1;
         r.swap = (fl >> 3) & 1;
@@ -770,7 +792,8 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
   unsigned npos;
   pair_signature(P, iBlk, jBlk, definite, npos);
   unsigned blk_s = 0u, blk_b = 0u;
-  inner64<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, blk_s, blk_b);
+  inner64<SORT>(R, Vl, s0, P.s0steps, P.nswp0, definite, npos, red, blk_s, blk_b,
+                reinterpret_cast<double *>(sm + kOffRot) + 16u * warp);
   if (rec)
     P.clk[3] = clock64() - t_start;
 
@@ -957,12 +980,14 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
     const unsigned ct = tid - 128u; // 0..127: row ct of the tile
     const bool lead = ct == 0u;
     // the lead's count of the asynchronous work it started and saw finish, for
-    // the drain on the failure path: tile loads per buffer, B loads, commits per half
-    unsigned l_iss[2] = {0u, 0u}, l_done[2] = {0u, 0u}, b_iss = 0u, b_done = 0u, m_iss[2] = {0u, 0u};
+    // the drain on the failure path: tile loads per buffer (issued, landed),
+    // B loads, commits per half -- scalars, so that they stay in registers
+    unsigned li0 = 0u, li1 = 0u, ld0 = 0u, ld1 = 0u, b_iss = 0u, b_done = 0u, mi0 = 0u, mi1 = 0u;
     if (lead)
       for (unsigned k = it0; k < it1 && k < it0 + 2u; ++k) {
         load_tile(P, item_of(P, k), sm + kOffUStage + (k - it0) * kUStage, &bar[kBarFull + (k - it0)]);
-        ++l_iss[k - it0];
+        li0 += (k == it0) ? 1u : 0u;
+        li1 += (k == it0) ? 0u : 1u;
       }
     auto col_word = [&](const Item &x) -> uint32_t {
       const unsigned gc = (ct < kBW) ? x.iBlk * kBW + ct : x.jBlk * kBW + ct - kBW;
@@ -992,7 +1017,8 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
       }
       if (ok) {
         ok = wait_or_abort(&bar[kBarFull + buf], (n >> 1) & 1u, abort_flag);
-        l_done[buf] += ok ? 1u : 0u;
+        ld0 += (ok && !buf) ? 1u : 0u;
+        ld1 += (ok && buf) ? 1u : 0u;
       }
       if (newb) {
         key = it.key;
@@ -1033,7 +1059,8 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
       if (lead) {
         if (k + 2u < it1) { // the tile is cut: its buffer takes the item two ahead
           load_tile(P, item_of(P, k + 2u), sm + kOffUStage + buf * kUStage, &bar[kBarFull + buf]);
-          ++l_iss[buf];
+          li0 += buf ? 0u : 1u;
+          li1 += buf ? 1u : 0u;
         }
         const uint64_t a0 = sdesc(sbase + kOffUA, 128u, 512u), b0 = sdesc(sbase + kOffUB, 128u, 512u);
 #pragma unroll
@@ -1052,7 +1079,8 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
                      b0 + ((h * kBHalf + kh * 256u) >> 4), idesc_i8(128u, 32u * (kDig - t)),
                      (t == 0u && kh == 0u) ? 0u : 1u);
           mma_commit(&bar[kBarMma + h]);
-          ++m_iss[h];
+          mi0 += h ? 0u : 1u;
+          mi1 += h ? 1u : 0u;
         }
       }
     }
@@ -1060,14 +1088,16 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
       // before the shared memory and TMEM are given up, what was started
       // completes (bounded): the tile loads and the B load not yet waited
       // for, and each half's last MMAs
-      for (unsigned b = 0u; b < 2u; ++b)
-        if (l_iss[b] > l_done[b])
-          (void)mbar_wait_bounded(&bar[kBarFull + b], (l_iss[b] - 1u) & 1u, kWait / 8);
+      if (li0 > ld0)
+        (void)mbar_wait_bounded(&bar[kBarFull], (li0 - 1u) & 1u, kWait / 8);
+      if (li1 > ld1)
+        (void)mbar_wait_bounded(&bar[kBarFull + 1u], (li1 - 1u) & 1u, kWait / 8);
       if (b_iss > b_done)
         (void)mbar_wait_bounded(&bar[kBarB], (b_iss - 1u) & 1u, kWait / 8);
-      for (unsigned h = 0u; h < 2u; ++h)
-        if (m_iss[h] > 0u)
-          (void)mbar_wait_bounded(&bar[kBarMma + h], (m_iss[h] - 1u) & 1u, kWait / 8);
+      if (mi0 > 0u)
+        (void)mbar_wait_bounded(&bar[kBarMma], (mi0 - 1u) & 1u, kWait / 8);
+      if (mi1 > 0u)
+        (void)mbar_wait_bounded(&bar[kBarMma + 1u], (mi1 - 1u) & 1u, kWait / 8);
     }
   }
   else {
