@@ -755,8 +755,31 @@ __global__ void __launch_bounds__(kThreads, 1) sp_pair_kernel(const __grid_const
         pivot(j);
       }
       else {
+        // the columns of a round are independent: three at a time, so that
+        // their shared-memory loads overlap (each entry's operations unchanged)
         const double l0 = R[k * kLd + lane], l1 = R[k * kLd + lane + 32u];
-        for (unsigned j = k + 1u + warp; j < 64u; j += 7u) {
+        unsigned j = k + 1u + warp;
+#pragma unroll 1
+        for (; j + 14u < 64u; j += 21u) {
+          double ljk[3], a0[3], a1[3];
+#pragma unroll
+          for (unsigned u = 0u; u < 3u; ++u) {
+            const unsigned jj = j + 7u * u;
+            ljk[u] = R[k * kLd + jj];
+            a0[u] = R[jj * kLd + lane];
+            a1[u] = R[jj * kLd + lane + 32u];
+          }
+#pragma unroll
+          for (unsigned u = 0u; u < 3u; ++u) {
+            const unsigned jj = j + 7u * u;
+            if (lane >= jj)
+              R[jj * kLd + lane] = __fma_rn(-l0, ljk[u], a0[u]);
+            if (lane + 32u >= jj)
+              R[jj * kLd + lane + 32u] = __fma_rn(-l1, ljk[u], a1[u]);
+          }
+        }
+#pragma unroll 1
+        for (; j < 64u; j += 7u) {
           const double ljk = R[k * kLd + j];
           if (lane >= j)
             R[j * kLd + lane] = __fma_rn(-l0, ljk, R[j * kLd + lane]);
