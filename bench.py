@@ -16,7 +16,9 @@ decomposition to convergence.  Metric: matrices per second (whole job).
   per block pair, 64 pairs) over its mean event-timed launch duration;
 * cpu_baseline: the CPU oracle port (OpenMP, all host threads) timed on the
   first outer steps of the same decomposition, scaled to a whole one; DGESVJ
-  (OpenBLAS, all host threads) on the full matrix is reported beside it.
+  (OpenBLAS, all host threads) on the full matrix is reported beside it
+  (--config c5: one SVD and one HSVD decomposition of each n by the port,
+  scaled by the batch's count of each n).
 
 N > 1: independent replicas (the single-matrix SVD is not sharded), barrier
 and max-over-ranks device time; value = matrices of all ranks / that time.
@@ -264,6 +266,31 @@ def ref_gpu_runs(G0: np.ndarray, m, n, nplus, alg, steps: int, warmup: int, budg
             "rot_s": out["rot_s"], "rot_b": out["rot_b"], "warmup": warm, "steps": len(runs), "build": REF_BUILD}
 
 
+def batch_cpu_sample(sizes, seed: int):
+    """The oracle port (all host threads) on the batch: one SVD (NPLUS = n)
+    and one HSVD (NPLUS = n/2) decomposition per n of the batch, scaled by the
+    batch's count of each n."""
+    from gpujachx_b200 import STRAT_PATH, synth
+    from oracle import oracle as O
+    O.build()
+    cores = os.cpu_count() or 1
+    s0 = O.load_strat(STRAT_PATH, "cycwor", 32)
+    tot, cpu_by = 0.0, {}
+    for n in sorted(set(int(x) for x in sizes)):
+        G = synth.make("svd_synth", n, n, seed + n, smin=1e-6)
+        s1 = O.load_strat(STRAT_PATH, "cycwor", n // 16)
+        per = 0.0
+        for npl in (n, n // 2):
+            t0 = time.perf_counter()
+            O.hypjac_l2(ALG, G, npl, s0, s1, nthreads=cores)
+            per += 0.5 * (time.perf_counter() - t0)
+        cpu_by[n] = per
+        tot += per * int((sizes == n).sum())
+    return {"value": len(sizes) / tot, "unit": "matrices/s", "cores": cores, "kind": "port",
+            "sample": "one SVD and one HSVD (NPLUS = n/2) per n by the oracle port, scaled by the batch's count "
+                      "of each n", "seconds_by_n": cpu_by}
+
+
 def reference_arm_batch(args):
     """c5 on the reference path: the reference's own sm_100a build has no
     batched form, so it is looped -- per batch size n, one SVD (NPLUS = n)
@@ -271,7 +298,7 @@ def reference_arm_batch(args):
     in one process (its compute phase and wall time), scaled by how many
     matrices of that n the batch holds.  The CPU oracle port, one
     decomposition of each, is reported beside it (cpu_baseline)."""
-    from gpujachx_b200 import STRAT_PATH, synth
+    from gpujachx_b200 import synth
     from tests.golden.make_golden import HARNESS, case, run_ref
     cfg = WORKLOADS["c5"]
     sizes = batch_sizes(cfg["count"], cfg["seed"])
@@ -307,28 +334,10 @@ def reference_arm_batch(args):
                     reference={"kind": "reference", "build": REF_BUILD, "by_n": by_n,
                                "sample": f"one SVD and one HSVD matrix per n, {reps} timed runs each after one "
                                          "warm-up run; one step = the batch, scaled from the per-n times"})
-    cpu = None
-    if not args.no_cpu:
-        from oracle import oracle as O
-        O.build()
-        cores = os.cpu_count() or 1
-        s0 = O.load_strat(STRAT_PATH, "cycwor", 32)
-        tot, cpu_by = 0.0, {}
-        for n in ns:
-            G = synth.make("svd_synth", n, n, cfg["seed"] + n, smin=1e-6)
-            s1 = O.load_strat(STRAT_PATH, "cycwor", n // 16)
-            per = 0.0
-            for npl in (n, n // 2):
-                t0 = time.perf_counter()
-                O.hypjac_l2(ALG, G, npl, s0, s1, nthreads=cores)
-                per += 0.5 * (time.perf_counter() - t0)
-            cpu_by[n] = per
-            tot += per * int((sizes == n).sum())
-        cpu = {"value": len(sizes) / tot, "unit": "matrices/s", "cores": cores, "kind": "port",
-               "sample": "one SVD and one HSVD (NPLUS = n/2) per n by the oracle port, scaled by the batch's count "
-                         "of each n", "seconds_by_n": cpu_by}
+    cpu = None if args.no_cpu else batch_cpu_sample(sizes, cfg["seed"])
     if line is None:
-        line = dict(base, value=cpu["value"], steps=1, steps_requested=args.steps, ms_per_step=1000.0 * tot,
+        line = dict(base, value=cpu["value"], steps=1, steps_requested=args.steps,
+                    ms_per_step=1000.0 * len(sizes) / cpu["value"],
                     e2e={"value": cpu["value"], "unit": "matrices/s", "h2d_bytes_per_step": 0,
                          "d2h_bytes_per_step": 0},
                     note="reference build absent: the CPU oracle port, scaled from one matrix of each n")
@@ -576,6 +585,7 @@ def main_batch(args):
             "clocks": clk, "gpu_launches": prof["launches"] // max(1, args.steps), "step_ms": times}
     if rank == 0 and world == 1 and not args.no_cpu:
         line["plain_loop"] = plain_loop_sample(Gs, Vs, Ds, G0, offs, sizes, nplus)
+        line["cpu_baseline"] = batch_cpu_sample(sizes, cfg["seed"])
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -50,8 +50,8 @@ Strat g_strat;
 int g_verbose = 1;
 int g_sweep_mode = -1; // -1 automatic (the tuned choice, else per step), 0 per outer step, 1 one launch per sweep
 unsigned g_split = 0u;  // CTAs per block pair: 0 automatic (the tuned choice, else by the SM count), else 1, 2, 4
-unsigned g_pairs_per_cta = 0u; // block pairs a CTA takes at a time: 0 automatic, 1, 2, or 3 (batched form:
-                               // one per CTA of 4 warps, two CTAs per SM)
+unsigned g_pairs_per_cta = 0u; // block pairs a CTA takes at a time: 0 automatic, 1, 2, or (batched form, two
+                               // CTAs of 4 warps per SM) 3: one per CTA, 4: two per CTA
 unsigned g_variant = 0u; // pivot-block factor: 0 Gram + Cholesky, 1 QR (-DUSE_QR), 2 QR + Drmac (-DUSE_DRMAC)
 int g_batch_mode = -1;   // batched form: -1 the tuned choice (else per step), 0 one launch per step, 1 per sweep
 unsigned g_batch_cap = 0u; // nonzero: the batched form stops after this many sweeps (the autotuner's runs)
@@ -1360,14 +1360,18 @@ int gjx_autotune_batched(const unsigned routine, const unsigned nmat, const unsi
   const unsigned saved_width = g_pairs_per_cta, saved_cap = g_batch_cap;
   g_batch_cap = sweeps ? sweeps : 1u;
   float best = 3.0e38f;
-  std::pair<unsigned, int> pick{2u, 0};
+  std::pair<unsigned, int> pick{gjx::kWidthHalf2, 0};
   int rc = 0;
-  for (unsigned width : {2u, 1u, gjx::kWidthHalf, gjx::kWidthHalf2}) {
+  // The capped sweeps weigh the first sweeps, where nearly every pair rotates; over a whole batch the
+  // forms that hold more pairs per CTA gain further (a batch of 4096 of n = 64...512 to convergence:
+  // two pairs per CTA of 4 warps 1116 matrices/s, one 986, two per CTA of 8 warps 892, one 703), so
+  // the forms are tried in that order, per-step launches first, and a later one must be 3 % faster.
+  for (unsigned width : {gjx::kWidthHalf2, gjx::kWidthHalf, 2u, 1u}) {
     for (int mode : {0, 1}) {
       g_pairs_per_cta = width;
       g_batch_mode = mode;
-      float ms = 0.0f;
-      for (int rep = 0; rep < 2 && !rc; ++rep) { // the first run warms up
+      float ms = 3.0e38f;
+      for (int rep = 0; rep < 3 && !rc; ++rep) { // the first run warms up; the faster of the other two counts
         if (cudaMemcpyAsync(g, g0, nG * sizeof(double), cudaMemcpyDeviceToDevice, nullptr) != cudaSuccess ||
             cudaEventRecord(e0, nullptr) != cudaSuccess) {
           rc = GJX_ERR_CUDA;
@@ -1375,13 +1379,16 @@ int gjx_autotune_batched(const unsigned routine, const unsigned nmat, const unsi
         }
         rc = run_batch(routine, nmat, nrow, ncol, nplus, pG.data(), ldG.data(), pV.data(), ldV.data(), pD.data(),
                        nullptr, swp.data(), s_.data(), b_.data(), info.data());
+        float t = 0.0f;
         if (!rc && (cudaEventRecord(e1, nullptr) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-                    cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+                    cudaEventElapsedTime(&t, e0, e1) != cudaSuccess))
           rc = GJX_ERR_CUDA;
+        if (!rc && rep)
+          ms = std::min(ms, t);
       }
       if (rc)
         break;
-      if (ms < best) {
+      if (ms < 0.97f * best || best > 1.0e38f) {
         best = ms;
         pick = {width, mode};
       }

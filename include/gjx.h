@@ -152,13 +152,15 @@ void gjx_autotune_clear(void);
  * previous step.  The results are the same bits either way. */
 void gjx_set_batch_mode(int mode);
 
-/* Autotuner of the batched form: times block pairs per CTA (2, 1, 3, 4) x launch
+/* Autotuner of the batched form: times block pairs per CTA (4, 3, 2, 1) x launch
  * mode (per step, per sweep) on seeded random matrices of the batch's shapes
  * (nrow[b] x ncol[b], the signature kind of nplus[b]), `sweeps` sweeps each
- * (0: 1), and uses the fastest in later gjx_hypJacL2_batched calls on a
- * batch of the same shapes (in any order) unless gjx_set_pairs_per_cta /
- * gjx_set_batch_mode fix them.  out[2] = {pairs per CTA, mode}.  0 or an
- * error code. */
+ * (0: 1; the faster of two runs after a warm-up run), and uses the fastest in
+ * later gjx_hypJacL2_batched calls on a batch of the same shapes (in any
+ * order) unless gjx_set_pairs_per_cta / gjx_set_batch_mode fix them.  A
+ * configuration later in that order must be 3 % faster to be taken: the first
+ * sweeps rank the forms closer together than whole batches do.  out[2] =
+ * {pairs per CTA, mode}.  0 or an error code. */
 int gjx_autotune_batched(unsigned routine, unsigned nmat, const unsigned *nrow, const unsigned *ncol,
                          const unsigned *nplus, unsigned sweeps, unsigned *out);
 
