@@ -15,8 +15,9 @@
 // library holds it (kScratchBytes) until the process exits.  In host code its
 // name is only a host-side stand-in, not a device address, so the address is
 // taken with cudaGetSymbolAddress, once per device, with that device current,
-// on the first call made on it; that first call should come before any stream
-// capture.  The set-up is repeated only when the device's CUDA context is not
+// on the first call made on it, which must not come while a stream of the
+// device is being captured.  No call can itself be captured: after every sweep
+// it reads the rotation counters back and synchronises its stream.  The set-up is repeated only when the device's CUDA context is not
 // the one it was made in (a caller's cudaDeviceReset destroys the context, and
 // the array and its address with it): the context's id is kept beside the
 // address, and the tables are uploaded again into the new array.  All calls

@@ -231,8 +231,10 @@ int gjx_hypJacL2_dev(const unsigned routine, const unsigned nrow, const unsigned
  * array held by every GPU that loads the library until the process exits;
  * the loaded outer table must fit it (n1 <= 512 blocks, ncol <= 8192), else
  * GJX_ERR_SCRATCH.  The first call on a device takes the array's address
- * (cudaGetSymbolAddress) with that device current; make it before any stream
- * capture.  All calls share the array: each clears its counters and rewrites
+ * (cudaGetSymbolAddress) with that device current; make it while no stream of
+ * the device is being captured.  No call can run inside a stream capture: after
+ * every sweep it reads the rotation counters back and synchronises its stream.
+ * All calls share the array: each clears its counters and rewrites
  * the tables when they or the device changed (or the device's context was
  * re-created); calls that overlap on the GPU race.  The call holds the
  * library's host lock until its result is ready, so other calls into the
