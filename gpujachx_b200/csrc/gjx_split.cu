@@ -92,7 +92,8 @@ struct Params {
   int gdefinite;
   int accv;
   unsigned sms; // CTAs of the persistent update grid
-  long long *clk; // block 0 of sp_pair_kernel: clock64 at the phase ends (gjx_split_phase_cycles)
+  long long *clk; // [0..4] block 0 of sp_pair_kernel: clock64 at the phase ends; [5..9] CTA 0 of
+                  // sp_update_kernel, sums over the call (gjx_split_phase_cycles)
 };
 
 // ---- the update's B operand in global memory: for each half of the output
@@ -1006,6 +1007,10 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
     // the drain on the failure path: tile loads per buffer (issued, landed),
     // B loads, commits per half -- scalars, so that they stay in registers
     unsigned li0 = 0u, li1 = 0u, ld0 = 0u, ld1 = 0u, b_iss = 0u, b_done = 0u, mi0 = 0u, mi1 = 0u;
+    // CTA 0's lead: cycles waiting for the tensor core or the epilogue (free planes, free TMEM),
+    // cutting, waiting for copies (tiles, B)
+    const bool timed = lead && blockIdx.x == 0u;
+    long long c_mma = 0, c_cut = 0, c_copy = 0, tc = 0;
     if (lead)
       for (unsigned k = it0; k < it1 && k < it0 + 2u; ++k) {
         load_tile(P, item_of(P, k), sm + kOffUStage + (k - it0) * kUStage, &bar[kBarFull + (k - it0)]);
@@ -1022,9 +1027,15 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
       const Item it = item_of(P, k);
       const unsigned buf = n & 1u;
       bool ok = true;
+      if (timed)
+        tc = clock64();
       // the previous item's MMAs are complete: A and B are free
       if (n > 0u)
         ok = wait_or_abort(&bar[kBarMma + 1u], (n - 1u) & 1u, abort_flag);
+      if (timed) {
+        c_mma += clock64() - tc;
+        tc = clock64();
+      }
       const bool newb = it.key != key;
       if (ok && newb && lead) {
         mbar_arrive_expect_tx(&bar[kBarB], kBopBytes);
@@ -1042,6 +1053,10 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
         ok = wait_or_abort(&bar[kBarFull + buf], (n >> 1) & 1u, abort_flag);
         ld0 += (ok && !buf) ? 1u : 0u;
         ld1 += (ok && buf) ? 1u : 0u;
+      }
+      if (timed) {
+        c_copy += clock64() - tc;
+        tc = clock64();
       }
       if (newb) {
         key = it.key;
@@ -1077,6 +1092,10 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
       }
       fence_async_shared();
       bar_sync(1u, 128u);
+      if (timed) {
+        c_cut += clock64() - tc;
+        tc = clock64();
+      }
       if (ct < 64u && k + 1u < it1)
         next_cmax = col_word(item_of(P, k + 1u));
       if (lead) {
@@ -1105,7 +1124,15 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
           mi0 += h ? 0u : 1u;
           mi1 += h ? 1u : 0u;
         }
+        if (timed)
+          c_mma += clock64() - tc;
       }
+    }
+    if (timed) {
+      atomicAdd(reinterpret_cast<unsigned long long *>(P.clk + 5), (unsigned long long)c_mma);
+      atomicAdd(reinterpret_cast<unsigned long long *>(P.clk + 6), (unsigned long long)c_cut);
+      atomicAdd(reinterpret_cast<unsigned long long *>(P.clk + 7), (unsigned long long)c_copy);
+      atomicAdd(reinterpret_cast<unsigned long long *>(P.clk + 9), (unsigned long long)(it1 - it0));
     }
     if (lead && *abort_flag) {
       // before the shared memory and TMEM are given up, what was started
@@ -1126,6 +1153,8 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
   else {
     // ------------------------------ epilogue -------------------------------
     const unsigned q4 = warp, r = q4 * 32u + lane; // TMEM lanes of this warp: the tile's rows
+    const bool etimed = tid == 0u && blockIdx.x == 0u;
+    long long c_epi = 0, te = 0;
     for (unsigned k = it0, n = 0u; k < it1; ++k, ++n) {
       const Item it = item_of(P, k);
       const unsigned buf = n & 1u;
@@ -1145,6 +1174,8 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
           break;
         }
         tc_fence_after();
+        if (etimed)
+          te = clock64();
         double *const colh = out + (size_t)((h ? it.jBlk : it.iBlk) * kBW) * ld + it.row0 + r;
 #pragma unroll 1
         for (unsigned ch = 0u; ch < 2u; ++ch) {
@@ -1173,6 +1204,8 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
         __syncwarp();
         if (lane == 0u)
           mbar_arrive(&bar[kBarFree + h]);
+        if (etimed)
+          c_epi += clock64() - te;
       }
       if (!ok)
         break;
@@ -1185,6 +1218,8 @@ __global__ void __launch_bounds__(kThreads, 1) sp_update_kernel(const __grid_con
       }
       bar_sync(2u, 128u);
     }
+    if (etimed)
+      atomicAdd(reinterpret_cast<unsigned long long *>(P.clk + 8), (unsigned long long)c_epi);
   }
   tc_fence_before();
   __syncthreads();

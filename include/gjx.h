@@ -269,9 +269,11 @@ int gjx_hypJacL2_split(const unsigned routine, const unsigned nrow, const unsign
  * 0's CTA in the last pair-kernel launch of the last gjx_hypJacL2_split call
  * to the end of [0] the Gram products, [1] the Gram epilogue, [2] the
  * Cholesky factor, [3] the inner sweeps, [4] the update's B operands; and
- * CTA 0 of the update kernel, summed over that call: [5] waiting for its
- * copies, [6] cutting tiles into digits, [7] the tensor-core products, [8] the
- * epilogues, [9] the tiles it took.  0 or GJX_ERR_CUDA. */
+ * CTA 0 of the update kernel, summed over that call (clock64 in one thread of
+ * each warp group): [5] the cutters waiting for the tensor core or the
+ * epilogue (digit planes or TMEM to be freed) and issuing the products, [6]
+ * cutting tiles into digits, [7] the cutters waiting for copies (tiles, B
+ * operands), [8] the epilogues, [9] the tiles it took.  0 or GJX_ERR_CUDA. */
 int gjx_split_phase_cycles(long long *out10);
 
 /* Frees the device buffers that hypJacL2 keeps between calls on the current
